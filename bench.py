@@ -1,0 +1,328 @@
+"""SpMMV HBM bandwidth on the 3D Anderson model, L=128 (n=2,097,152,
+nnz=14,680,064), stored as SELL-32-sigma (sigma=256), FP64, row-major block
+vectors of width nvec in {1,2,4,8,16,32}.
+
+One step = one SpMMV Y = A X for every nvec of the sweep (the kernel sweep of
+the benchmark configuration).  The metric is algorithmic bytes / device time,
+summed over the sweep:
+    bytes(nvec) = nnz*(8+4) + 8*n*nvec*2 + ceil(n/C)*(8+4)     (beta = 0)
+(the SpMMV byte model of PHIST, src/kernels/phist_kernel_perfmodels.hpp:92-107,
+with the block-vector term multiplied by nvec).
+
+    python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference]
+
+--impl reference times the CPU restatement of PHIST's builtin SpMMV
+(oracle/, the same loop order as spmvm_kernels.F90; PHIST's own kernels are
+Fortran+MPI and are not buildable here) on all host cores, on a bounded
+sample of the same workload.  Under torchrun only rank 0 runs that arm.
+"""
+import argparse
+import json
+import os
+import subprocess
+import sys
+import threading
+import time
+
+import numpy as np
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, ROOT)
+
+L = 128
+PROBLEM = "ANDERSON3D-%d-S1" % L
+NVECS = [1, 2, 4, 8, 16, 32]
+C_SELL = 32
+SIGMA = 256
+METRIC = "SpMMV HBM GB/s (algorithmic bytes / device time), FP64 SELL-32-256, nvec sweep 1..32"
+UNIT = "GB/s"
+
+
+def spmv_bytes(n, nnz, nvec, C=C_SELL):
+    nch = -(-n // C)
+    return nnz * 12 + 8 * n * nvec * 2 + nch * 12
+
+
+def read_peaks():
+    p = os.path.join(ROOT, "MEASURED_PEAKS.json")
+    try:
+        with open(p) as f:
+            d = json.load(f)
+        return float(d["hbm_gbs"]), "measured"
+    except Exception:
+        return 6650.0, "fallback"
+
+
+class ClockSampler:
+    """nvidia-smi samples of SM clock and throttle reasons during the timed region"""
+    Q = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+         "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+         "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, dev):
+        self.dev = dev
+        self.proc = None
+        self.lines = []
+
+    def start(self):
+        try:
+            self.proc = subprocess.Popen(
+                ["nvidia-smi", "-i", str(self.dev), "--query-gpu=" + self.Q, "--format=csv,noheader,nounits",
+                 "-lms", "100"], stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)
+            self.t = threading.Thread(target=self._read, daemon=True)
+            self.t.start()
+        except Exception:
+            self.proc = None
+
+    def _read(self):
+        for line in self.proc.stdout:
+            self.lines.append(line.strip())
+
+    def stop(self):
+        if self.proc is None:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["nvidia-smi unavailable"]}
+        time.sleep(0.25)
+        self.proc.terminate()
+        try:
+            self.proc.wait(timeout=5)
+        except Exception:
+            self.proc.kill()
+        sm, smax, reasons = [], None, set()
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        for l in self.lines:
+            f = [x.strip() for x in l.split(",")]
+            if len(f) < 9:
+                continue
+            try:
+                sm.append(float(f[1]))
+                smax = float(f[2])
+            except ValueError:
+                continue
+            for nm, val in zip(names, f[5:9]):
+                if val.lower().startswith("active"):
+                    reasons.add(nm)
+        return {"sm_mhz": float(np.median(sm)) if sm else None, "sm_max_mhz": smax,
+                "reasons": sorted(reasons), "samples": len(sm)}
+
+
+def cpu_baseline(steps_budget_s=12.0, nvecs=NVECS):
+    """oracle SpMMV (CPU restatement of the builtin loop) on all host cores"""
+    from oracle import oracle as O
+    from phist_b200 import generators as G
+    O.set_threads(os.cpu_count() or 1)
+    rp, c, v = G.anderson3d(L, 1)
+    n = len(rp) - 1
+    nnz = int(rp[-1])
+    xs = {k: G.random_block(n, k, 3) for k in nvecs}
+    ys = {k: np.zeros((n, k)) for k in nvecs}
+    lib = O.lib()
+    P = O._p
+    # warm-up
+    for k in nvecs:
+        lib.orc_spmmv(n, P(rp), P(c), P(v), k, 1.0, None, P(xs[k]), k, 0.0, P(ys[k]), k)
+    total_b, total_t, passes = 0.0, 0.0, 0
+    t_end = time.perf_counter() + steps_budget_s
+    while passes < 1 or time.perf_counter() < t_end:
+        for k in nvecs:
+            t0 = time.perf_counter()
+            lib.orc_spmmv(n, P(rp), P(c), P(v), k, 1.0, None, P(xs[k]), k, 0.0, P(ys[k]), k)
+            total_t += time.perf_counter() - t0
+            total_b += spmv_bytes(n, nnz, k)
+        passes += 1
+        if passes >= 50:
+            break
+    return {"value": round(total_b / total_t / 1e9, 3), "unit": UNIT, "cores": O.num_threads(),
+            "kind": "port",
+            "sample": "%d full passes of the nvec sweep {%s} on the same L=128 Anderson matrix (CRS, "
+                      "columns sorted), C restatement of PHIST builtin dspmvm (spmvm_kernels.F90:494-523), "
+                      "OpenMP static over rows; bit-identical to PHIST's own nvec<=8 C kernels in tests"
+                      % (passes, ",".join(map(str, nvecs))),
+            "seconds": round(total_t, 3)}
+
+
+def run_reference(args, rank, world):
+    if rank != 0:
+        return 0
+    cb = cpu_baseline(steps_budget_s=max(3.0, 2.0 * args.steps))
+    line = {"impl": "reference", "metric": METRIC, "value": cb["value"], "unit": UNIT,
+            "n_gpus": world, "steps": args.steps, "warmup": args.warmup,
+            "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f64",
+            "data": "synthetic (seeded generator, ANDERSON3D L=128 seed 1)",
+            "config": {"workload": "spmmv_anderson3d_L128_nvec_sweep", "problem": PROBLEM,
+                       "n": L ** 3, "nnz": 7 * L ** 3, "nvec": NVECS, "format": "CRS (host)"},
+            "cpu_baseline": {k: cb[k] for k in ("value", "unit", "cores", "kind", "sample")},
+            "e2e": {"value": cb["value"], "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
+    print(json.dumps(line), flush=True)
+    return 0
+
+
+def main():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=5)
+    ap.add_argument("--warmup", type=int, default=3)
+    ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
+    ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--nvecs", default=",".join(map(str, NVECS)))
+    args = ap.parse_args()
+    nvecs = [int(t) for t in args.nvecs.split(",")]
+
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    rank = int(os.environ.get("RANK", "0"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    dist = None
+    if world > 1:
+        import datetime
+
+        import torch
+        import torch.distributed as dist
+        torch.cuda.set_device(local)
+        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=300))
+
+    if args.impl == "reference":
+        rc = run_reference(args, rank, world)
+        if dist is not None:
+            dist.destroy_process_group()
+        return rc
+
+    import torch
+
+    from phist_b200 import kernels as K
+    from phist_b200.objects import Mvec, SparseMat, launch_count, stream_handle
+
+    torch.cuda.set_device(local)
+    K.chk(K.phist_b200_set_sell_params, C_SELL, SIGMA)
+    A = SparseMat.from_problem(PROBLEM, flags=K.PHIST_SPARSEMAT_PERM_LOCAL)
+    n, nnz = A.nrows, A.nnz
+    info = A.sell_info()
+    lib_stream = torch.cuda.ExternalStream(stream_handle())
+    from phist_b200 import generators as G
+    X = {k: Mvec(A.domain_map, k).set(G.random_block(n, k, 3)) for k in nvecs}
+    Y = {k: Mvec(A.row_map, k) for k in nvecs}
+    flush = torch.empty(256 << 20, dtype=torch.uint8, device="cuda")  # 256 MiB > 126 MB L2
+
+    def one_step(times):
+        for k in nvecs:
+            with torch.cuda.stream(lib_stream):
+                flush.fill_(k & 0xFF)  # evict L2 (untimed)
+                e0 = torch.cuda.Event(enable_timing=True)
+                e1 = torch.cuda.Event(enable_timing=True)
+                e0.record(lib_stream)
+            K.chk(K.phist_DsparseMat_times_mvec, 1.0, A.h, X[k].h, 0.0, Y[k].h)
+            e1.record(lib_stream)
+            times.append((k, e0, e1))
+
+    for _ in range(args.warmup):
+        one_step([])
+    torch.cuda.synchronize()
+    if dist is not None:
+        dist.barrier()
+    torch.cuda.synchronize()
+    clocks = ClockSampler(local)
+    clocks.start()
+    l0 = launch_count()
+    ev = []
+    t_wall = time.perf_counter()
+    for _ in range(args.steps):
+        one_step(ev)
+    torch.cuda.synchronize()
+    t_wall = time.perf_counter() - t_wall
+    launches = launch_count() - l0
+    clk = clocks.stop()
+    per = {k: 0.0 for k in nvecs}
+    for k, e0, e1 in ev:
+        per[k] += e0.elapsed_time(e1) * 1e-3
+    dev_time = sum(per.values())
+    if dist is not None:
+        t = torch.tensor([dev_time], device="cuda", dtype=torch.float64)
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+        dev_time = float(t.item())
+        dist.barrier()
+    step_bytes = sum(spmv_bytes(n, nnz, k) for k in nvecs)
+    value = world * step_bytes * args.steps / dev_time / 1e9
+    detail = {str(k): round(spmv_bytes(n, nnz, k) * args.steps / per[k] / 1e9, 1) for k in nvecs}
+
+    # ---- end to end through the C ABI with pinned host buffers -------------
+    hx = {k: torch.from_numpy(G.random_block(n, k, 3)).pin_memory() for k in nvecs}
+    hy = {k: torch.empty((n, k), dtype=torch.float64).pin_memory() for k in nvecs}
+    h2d = sum(8 * n * k for k in nvecs)
+    d2h = h2d
+
+    def e2e_step():
+        for k in nvecs:
+            K.chk(K.phist_Dmvec_set_data, X[k].h, ct_ptr(hx[k]), k, 1)
+            K.chk(K.phist_DsparseMat_times_mvec, 1.0, A.h, X[k].h, 0.0, Y[k].h)
+            K.chk(K.phist_Dmvec_get_data, Y[k].h, ct_ptr(hy[k]), k, 1)
+
+    import ctypes
+
+    def ct_ptr(t):
+        return ctypes.c_void_p(t.data_ptr())
+
+    e2e_step()
+    torch.cuda.synchronize()
+    e0 = torch.cuda.Event(enable_timing=True)
+    e1 = torch.cuda.Event(enable_timing=True)
+    e0.record(lib_stream)
+    for _ in range(args.steps):
+        e2e_step()
+    e1.record(lib_stream)
+    torch.cuda.synchronize()
+    e2e_time = e0.elapsed_time(e1) * 1e-3
+    if dist is not None:
+        t = torch.tensor([e2e_time], device="cuda", dtype=torch.float64)
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+        e2e_time = float(t.item())
+    e2e_val = world * step_bytes * args.steps / e2e_time / 1e9
+    ok = np.isfinite(hy[nvecs[-1]].numpy()).all()
+
+    peak, peak_kind = read_peaks()
+    traffic = None
+    tp = os.path.join(ROOT, "profiles", "spmmv_traffic.json")
+    if os.path.exists(tp):
+        try:
+            with open(tp) as f:
+                traffic = json.load(f)
+        except Exception:
+            traffic = None
+
+    line = {
+        "metric": METRIC, "value": round(value, 2), "unit": UNIT, "n_gpus": world,
+        "steps": args.steps, "warmup": args.warmup,
+        "ms_per_step": round(dev_time / args.steps * 1e3, 4),
+        "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f64",
+        "data": "synthetic (seeded counter-based generator: 3D Anderson L=128 periodic, on-site U[-8.25,8.25] seed 1; X uniform[-1,1) seed 3)",
+        "config": {"workload": "spmmv_anderson3d_L128_nvec_sweep", "problem": PROBLEM, "n": n, "nnz": nnz,
+                   "format": "SELL-%d-%d" % (info["C"], info["sigma"]), "nnz_padded": info["nnz_padded"],
+                   "nvec": nvecs, "beta": 0.0, "parallelism": "replicas" if world > 1 else "single",
+                   "l2": "flushed before every SpMMV (256 MiB write, outside the timed events)"},
+        "per_nvec_gbs": detail,
+        "roofline": {"bound": "hbm", "kernel": "k_sell_spmmv (all nvec instantiations)",
+                     "achieved": round(step_bytes * args.steps / dev_time / 1e9, 2),
+                     "peak": peak, "peak_kind": peak_kind + " (MEASURED_PEAKS.json hbm_gbs, copy)",
+                     "unit": "GB/s", "frac": round(step_bytes * args.steps / dev_time / 1e9 / peak, 4),
+                     "traffic": traffic.get("bytes_per_step") if traffic else None,
+                     "algorithmic_bytes_per_step": step_bytes},
+        "e2e": {"value": round(e2e_val, 2), "unit": UNIT, "h2d_bytes_per_step": h2d, "d2h_bytes_per_step": d2h,
+                "path": "phist_Dmvec_set_data (pinned) -> phist_DsparseMat_times_mvec -> phist_Dmvec_get_data (pinned)"},
+        "gpu_launches": launches,
+        "clocks": clk,
+        "wall_s_timed": round(t_wall, 4),
+        "finite": bool(ok),
+    }
+    if rank == 0 and world == 1 and not args.no_cpu_baseline:
+        line["cpu_baseline"] = {k: v for k, v in cpu_baseline(steps_budget_s=12.0, nvecs=nvecs).items()
+                                if k != "seconds"}
+    if rank == 0:
+        print(json.dumps(line), flush=True)
+    for k in nvecs:
+        X[k].delete()
+        Y[k].delete()
+    A.delete()
+    if dist is not None:
+        dist.destroy_process_group()
+    return 0
+
+
+if __name__ == "__main__":
+    sys.exit(main())

@@ -1,0 +1,282 @@
+"""ctypes wrapper of the CPU oracle (TEST INFRASTRUCTURE ONLY).
+
+Loads oracle/liboracle.so (this project's C restatement of PHIST's builtin
+kernels, phist_oracle.c) and, when present, oracle/_ref/libref_builtin*.so
+(PHIST's own C kernels compiled from the PHIST sources by oracle/Makefile).
+Only the tests, the smoke check and bench.py's CPU-baseline leg use it; the
+library under test never does.
+
+All arrays are numpy; row-major block vectors (n x m, C order) and
+column-major small matrices (Fortran order) as in PHIST.
+"""
+import ctypes as ct
+import os
+import subprocess
+
+import numpy as np
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+LIB = os.path.join(HERE, "liboracle.so")
+REF = os.path.join(HERE, "_ref", "libref_builtin.so")
+REF_PREC = os.path.join(HERE, "_ref", "libref_builtin_prec.so")
+
+
+def build(with_ref=None):
+    """make -C oracle [ref]; ref only when the PHIST sources are reachable"""
+    targets = ["all"]
+    src = os.environ.get("PHIST_SRC", "/root/reference")
+    if with_ref is None:
+        with_ref = os.path.isdir(os.path.join(src, "src", "kernels", "builtin"))
+    if with_ref:
+        targets.append("ref")
+    subprocess.run(["make", "-s", "-C", HERE] + targets, check=True,
+                   env=dict(os.environ, PHIST_SRC=src))
+
+
+_lib = None
+
+
+def lib():
+    global _lib
+    if _lib is None:
+        if not os.path.exists(LIB):
+            build(with_ref=False)
+        _lib = ct.CDLL(LIB)
+        i64, i32, d, vp = ct.c_int64, ct.c_int, ct.c_double, ct.c_void_p
+        f = ct.c_float
+        _lib.orc_spmmv.argtypes = [i64, vp, vp, vp, i32, d, vp, vp, i64, d, vp, i64]
+        _lib.orc_sspmmv.argtypes = [i64, vp, vp, vp, i32, f, vp, vp, i64, f, vp, i64]
+        _lib.orc_mvTmv.argtypes = [i64, i32, i32, d, vp, i64, vp, i64, d, vp, i64]
+        _lib.orc_mvTmv_prec.argtypes = _lib.orc_mvTmv.argtypes
+        _lib.orc_mvsd.argtypes = [i64, i32, i32, d, vp, i64, vp, i64, d, vp, i64]
+        _lib.orc_mvsdi.argtypes = [i64, i32, i32, vp, i64, vp, i64]
+        _lib.orc_mvsd_add_mvsd.argtypes = [i64, i32, i32, vp, i64, vp, i64, vp, i64, vp, i64]
+        _lib.orc_fused_mvsd_mvTmv.argtypes = [i64, i32, i32, d, vp, i64, vp, i64, d, vp, i64, vp, i64]
+        _lib.orc_fused_mvsdi_mvTmv.argtypes = [i64, i32, i32, i32, d, vp, i64, vp, i64, vp, i64, d, vp, i64]
+        _lib.orc_dot.argtypes = [i64, i32, vp, i64, vp, i64, vp]
+        _lib.orc_dot_prec.argtypes = _lib.orc_dot.argtypes
+        _lib.orc_norm2.argtypes = [i64, i32, vp, i64, vp]
+        _lib.orc_vadd.argtypes = [i64, i32, d, vp, vp, i64, d, vp, i64]
+        _lib.orc_kacz_sweep.argtypes = [i64, vp, vp, vp, i32, vp, vp, i64, vp, i64, vp, vp, i64]
+        _lib.orc_carp_sweep.argtypes = [i64, vp, vp, vp, i32, vp, vp, i64, vp, i64, vp]
+        _lib.orc_sell_perm.argtypes = [i64, vp, i64, vp]
+        _lib.orc_check_dist2.argtypes = [i64, vp, vp, i64, vp]
+        _lib.orc_check_dist2.restype = i64
+        _lib.orc_set_num_threads.argtypes = [i32]
+        _lib.orc_num_threads.restype = i32
+    return _lib
+
+
+def _p(a):
+    return None if a is None else a.ctypes.data_as(ct.c_void_p)
+
+
+def _rows(a):
+    return a.shape[0]
+
+
+def set_threads(n):
+    lib().orc_set_num_threads(int(n))
+
+
+def num_threads():
+    return lib().orc_num_threads()
+
+
+def spmmv(rowptr, col, val, x, alpha=1.0, beta=0.0, y=None, shifts=None):
+    """Y = alpha (A + diag(shifts)) X + beta Y (row-major X, Y)"""
+    x = np.ascontiguousarray(x)
+    n = len(rowptr) - 1
+    nvec = x.shape[1]
+    if y is None:
+        y = np.zeros((n, nvec), x.dtype)
+    else:
+        y = np.array(y, dtype=x.dtype, order="C", copy=True)
+    sh = None if shifts is None else np.ascontiguousarray(shifts, x.dtype)
+    if x.dtype == np.float32:
+        lib().orc_sspmmv(n, _p(rowptr), _p(col), _p(np.ascontiguousarray(val, np.float32)), nvec,
+                         alpha, _p(sh), _p(x), nvec, beta, _p(y), nvec)
+    else:
+        lib().orc_spmmv(n, _p(rowptr), _p(col), _p(np.ascontiguousarray(val, np.float64)), nvec,
+                        alpha, _p(sh), _p(x), nvec, beta, _p(y), nvec)
+    return y
+
+
+def mvTmv(V, W, alpha=1.0, beta=0.0, C=None, prec=False):
+    V = np.ascontiguousarray(V, np.float64)
+    W = np.ascontiguousarray(W, np.float64)
+    m, k = V.shape[1], W.shape[1]
+    C = np.zeros((m, k), order="F") if C is None else np.array(C, order="F", dtype=np.float64)
+    f = lib().orc_mvTmv_prec if prec else lib().orc_mvTmv
+    f(V.shape[0], m, k, alpha, _p(V), m, _p(W), k, beta, _p(C), m)
+    return C
+
+
+def mvsd(V, C, alpha=1.0, beta=0.0, W=None):
+    V = np.ascontiguousarray(V, np.float64)
+    C = np.asfortranarray(C, np.float64)
+    n, m = V.shape
+    k = C.shape[1]
+    W = np.zeros((n, k)) if W is None else np.array(W, dtype=np.float64, order="C", copy=True)
+    lib().orc_mvsd(n, m, k, alpha, _p(V), m, _p(C), m, beta, _p(W), k)
+    return W
+
+
+def mvsdi(V, M):
+    V = np.array(V, dtype=np.float64, order="C", copy=True)
+    M = np.asfortranarray(M, np.float64)
+    n, m = V.shape
+    lib().orc_mvsdi(n, m, M.shape[1], _p(V), m, _p(M), m)
+    return V
+
+
+def mvsd_add_mvsd(V, C, W, D):
+    V = np.ascontiguousarray(V, np.float64)
+    W = np.array(W, dtype=np.float64, order="C", copy=True)
+    C = np.asfortranarray(C, np.float64)
+    D = np.asfortranarray(D, np.float64)
+    n, m = V.shape
+    k = W.shape[1]
+    lib().orc_mvsd_add_mvsd(n, m, k, _p(V), m, _p(C), m, _p(W), k, _p(D), k)
+    return W
+
+
+def fused_mvsd_mvTmv(V, C, W, alpha=1.0, beta=0.0):
+    V = np.ascontiguousarray(V, np.float64)
+    W = np.array(W, dtype=np.float64, order="C", copy=True)
+    C = np.asfortranarray(C, np.float64)
+    n, m = V.shape
+    k = W.shape[1]
+    G = np.zeros((k, k), order="F")
+    lib().orc_fused_mvsd_mvTmv(n, m, k, alpha, _p(V), m, _p(C), m, beta, _p(W), k, _p(G), k)
+    return W, G
+
+
+def fused_mvsdi_mvTmv(V, W, C, alpha=1.0, beta=0.0, D=None):
+    V = np.ascontiguousarray(V, np.float64)
+    W = np.array(W, dtype=np.float64, order="C", copy=True)
+    C = np.asfortranarray(C, np.float64)
+    n, mv = V.shape
+    m = W.shape[1]
+    k = C.shape[1]
+    D = np.zeros((mv, k), order="F") if D is None else np.array(D, order="F", dtype=np.float64)
+    lib().orc_fused_mvsdi_mvTmv(n, mv, m, k, alpha, _p(V), mv, _p(W), m, _p(C), m, beta, _p(D), mv)
+    return W[:, :k], D
+
+
+def dot(V, W, prec=False):
+    V = np.ascontiguousarray(V, np.float64)
+    W = np.ascontiguousarray(W, np.float64)
+    out = np.zeros(V.shape[1])
+    f = lib().orc_dot_prec if prec else lib().orc_dot
+    f(V.shape[0], V.shape[1], _p(V), V.shape[1], _p(W), W.shape[1], _p(out))
+    return out
+
+
+def kacz_sweep(rowptr, col, val, shifts, b, x, omega, order):
+    x = np.array(x, dtype=np.float64, order="C", copy=True)
+    nvec = x.shape[1]
+    bb = None if b is None else np.ascontiguousarray(b, np.float64)
+    order = np.ascontiguousarray(order, np.int32)
+    lib().orc_kacz_sweep(len(rowptr) - 1, _p(rowptr), _p(col), _p(np.ascontiguousarray(val, np.float64)),
+                         nvec, _p(np.ascontiguousarray(shifts, np.float64)), _p(bb), nvec, _p(x), nvec,
+                         _p(np.ascontiguousarray(omega, np.float64)), _p(order), len(order))
+    return x
+
+
+def carp_sweep(rowptr, col, val, shifts, b, x, omega, order=None):
+    """forward sweep over `order` (default 0..n-1), then backward over its reverse"""
+    n = len(rowptr) - 1
+    order = np.arange(n, dtype=np.int32) if order is None else np.asarray(order, np.int32)
+    x = kacz_sweep(rowptr, col, val, shifts, b, x, omega, order)
+    return kacz_sweep(rowptr, col, val, shifts, b, x, omega, order[::-1].copy())
+
+
+def sell_perm(rowptr, sigma):
+    n = len(rowptr) - 1
+    perm = np.zeros(n, np.int32)
+    lib().orc_sell_perm(n, _p(rowptr), sigma, _p(perm))
+    return perm
+
+
+def check_dist2(rowptr, col, ncols, color):
+    color = np.ascontiguousarray(color, np.int32)
+    return lib().orc_check_dist2(len(rowptr) - 1, _p(rowptr), _p(col), ncols, _p(color))
+
+
+# ------------------------------------------------ PHIST's own C kernels
+_ref = None
+_refp = None
+
+
+def ref_available():
+    return os.path.exists(REF) and os.path.exists(REF_PREC)
+
+
+def ref_libs():
+    """(plain, prec) handles of PHIST's builtin C kernels compiled from source"""
+    global _ref, _refp
+    if _ref is None:
+        _ref = ct.CDLL(REF)
+        _refp = ct.CDLL(REF_PREC)
+    return _ref, _refp
+
+
+def ref_spmmv_nt(rowptr, col, val, x, alpha=1.0, shifts=None, prec=False):
+    """PHIST's dspmvm_nt_<nvec>_c / dspmvm_nt_strided_<nvec>_c (beta = 0).
+
+    The kernels take Fortran (1-based) row offsets and column indices, a
+    separate halo offset (= row end with one process) and 16-byte aligned
+    output."""
+    plain, precl = ref_libs()
+    L = precl if prec else plain
+    n = len(rowptr) - 1
+    nvec = x.shape[1]
+    rp1 = np.ascontiguousarray(rowptr + 1, np.int64)
+    halo = np.ascontiguousarray(rowptr[1:] + 1, np.int64)
+    col1 = np.ascontiguousarray(col + 1, np.int32)
+    val = np.ascontiguousarray(val, np.float64)
+    sh = np.zeros(nvec) if shifts is None else np.ascontiguousarray(shifts, np.float64)
+    # 64-byte aligned buffers
+    def aligned(shape):
+        nb = int(np.prod(shape)) * 8
+        raw = np.zeros(nb + 64, np.uint8)
+        off = (-raw.ctypes.data) % 64
+        return raw[off:off + nb].view(np.float64).reshape(shape)
+    xa = aligned(x.shape)
+    xa[...] = x
+    ya = aligned((n, nvec))
+    hal = np.zeros(8)
+    d, i32 = ct.c_double, ct.c_int
+    if nvec == 1:
+        f = L.dspmvm_nt_1_c
+        f.argtypes = [i32, d] + [ct.c_void_p] * 8
+        f(n, alpha, _p(rp1), _p(halo), _p(col1), _p(val), _p(sh), _p(xa), _p(hal), _p(ya))
+    else:
+        f = getattr(L, "dspmvm_nt_strided_%d_c" % nvec)
+        f.argtypes = [i32, d] + [ct.c_void_p] * 6 + [i32, ct.c_void_p, ct.c_void_p, i32]
+        f(n, alpha, _p(rp1), _p(halo), _p(col1), _p(val), _p(sh), _p(xa), nvec, _p(hal), _p(ya), nvec)
+    return np.array(ya)
+
+
+def ref_ddot_prec(x, y):
+    """PHIST's compensated dot (ddot_prec_<nvec>, dot_kernels_prec.c), nvec 1|2|4"""
+    _, precl = ref_libs()
+    # the kernels assume the row count padded to a multiple of 4 with zeros
+    pad = (-x.shape[0]) % 4
+    x = np.vstack([x, np.zeros((pad, x.shape[1]))])
+    y = np.vstack([y, np.zeros((pad, y.shape[1]))])
+    n, nvec = x.shape
+    res = np.zeros(nvec)
+    resC = np.zeros(nvec)
+    raw = [np.zeros(x.size * 8 + 64, np.uint8) for _ in range(2)]
+    bufs = []
+    for r, a in zip(raw, (x, y)):
+        off = (-r.ctypes.data) % 64
+        b = r[off:off + a.size * 8].view(np.float64).reshape(a.shape)
+        b[...] = a
+        bufs.append(b)
+    f = getattr(precl, "ddot_prec_%d" % nvec)
+    f.argtypes = [ct.c_int] + [ct.c_void_p] * 4
+    f(n, _p(bufs[0]), _p(bufs[1]), _p(res), _p(resC))
+    return res, resC

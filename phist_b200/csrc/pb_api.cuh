@@ -1,0 +1,911 @@
+// pb_api.cuh -- typed implementation of the phist_kernels C API
+// (phist_kernels_decl.h, phist_kernels_common_decl.h,
+// phist_kernels_fused_decl.h, phist_kernels_carp_decl.h).  Instantiated for
+// double (phist_D*) in pb_api_D.cu and float (phist_S*) in pb_api_S.cu.
+#pragma once
+#include <algorithm>
+#include <cmath>
+#include <numeric>
+
+#include "pb_blas.cuh"
+#include "pb_block.cuh"
+#include "pb_carp.cuh"
+#include "pb_core.hpp"
+#include "pb_spmmv.cuh"
+
+namespace pb {
+
+inline int grid_for(int64_t work, int bs = 256)
+{
+  int64_t g = ceil_div(work > 0 ? work : 1, bs);
+  int64_t cap = (int64_t)rt().num_sms() * 16;
+  return (int)(g < cap ? g : cap);
+}
+
+template <class T>
+inline Mvec<T>* MV(const void* p)
+{
+  PB_REQUIRE(p, PB_BAD_CAST, "mvec handle is NULL");
+  return (Mvec<T>*)p;
+}
+template <class T>
+inline SdMat<T>* SD(const void* p)
+{
+  PB_REQUIRE(p, PB_BAD_CAST, "sdMat handle is NULL");
+  return (SdMat<T>*)p;
+}
+template <class T>
+inline SparseMat<T>* SP(const void* p)
+{
+  PB_REQUIRE(p, PB_BAD_CAST, "sparseMat handle is NULL");
+  return (SparseMat<T>*)p;
+}
+
+inline void ensure_init()
+{
+  if (!rt().initialized()) rt().init();
+}
+
+// ======================================================================
+// mvec object model
+// ======================================================================
+template <class T>
+void mvec_create(void** V, const void* vmap, int nvec, int flags)
+{
+  (void)flags;
+  ensure_init();
+  PB_REQUIRE(V && vmap, PB_BAD_CAST, "NULL argument");
+  PB_REQUIRE(nvec >= 1, PB_INVALID_INPUT, "nvec must be >= 1, got %d", nvec);
+  const Map* map = (const Map*)vmap;
+  Mvec<T>* v = new Mvec<T>();
+  v->map = map;
+  v->nrows = map->nloc;
+  v->nvec = nvec;
+  v->lda = nvec;
+  v->root = v;
+  v->col_off = 0;
+  size_t bytes = sizeof(T) * (size_t)nvec * (size_t)(map->nloc > 0 ? map->nloc : 1);
+  try {
+    v->d_base = (T*)rt().dmalloc(bytes);
+  } catch (...) {
+    delete v;
+    throw;
+  }
+  // new objects are zero, as the builtin allocation touches them with zeros
+  PB_CUDA(cudaMemsetAsync(v->d_base, 0, bytes, stream()));
+  *V = v;
+}
+
+template <class T>
+void mvec_delete(void* vV)
+{
+  if (!vV) return;
+  Mvec<T>* v = (Mvec<T>*)vV;
+  if (!v->is_view()) {
+    rt().dfree(v->d_base);
+    free(v->h_base);
+  }
+  delete v;
+}
+
+template <class T>
+void mvec_view_block(void* vV, void** vblock, int jmin, int jmax)
+{
+  Mvec<T>* V = MV<T>(vV);
+  PB_REQUIRE(vblock, PB_BAD_CAST, "Vblock is NULL");
+  PB_REQUIRE(jmin >= 0 && jmax < V->nvec && jmin <= jmax, PB_INVALID_INPUT,
+             "view columns %d:%d out of range for %d columns", jmin, jmax, V->nvec);
+  Mvec<T>* b = (Mvec<T>*)*vblock;
+  if (b && !b->is_view()) {
+    mvec_delete<T>(b);
+    b = nullptr;
+  }
+  if (!b) b = new Mvec<T>();
+  b->map = V->map;
+  b->nrows = V->nrows;
+  b->nvec = jmax - jmin + 1;
+  b->lda = V->lda;
+  b->root = V->root;
+  b->col_off = V->col_off + jmin;
+  b->d_base = nullptr;
+  b->h_base = nullptr;
+  *vblock = b;
+}
+
+template <class T>
+void copy_cols(const Mvec<T>* X, int xoff, Mvec<T>* Y, int yoff, int ncols)
+{
+  if (X->nrows == 0 || ncols == 0) return;
+  k_copy<T, T><<<grid_for((int64_t)X->nrows * ncols), 256, 0, stream()>>>(
+      X->d() + xoff, X->lda, Y->d() + yoff, Y->lda, X->nrows, ncols);
+  PB_LAUNCH_CHECK();
+}
+
+template <class T>
+void check_same_rows(const Mvec<T>* a, const Mvec<T>* b)
+{
+  PB_REQUIRE(a->nrows == b->nrows, PB_INVALID_INPUT, "mvecs have %d and %d rows", a->nrows,
+             b->nrows);
+}
+
+// host mirror <-> device for the columns of a view
+template <class T>
+void mvec_upload(Mvec<T>* V)
+{
+  if (V->nrows == 0) return;
+  T* h = V->h();
+  PB_CUDA(cudaMemcpy2DAsync(V->d(), V->lda * sizeof(T), h, V->lda * sizeof(T),
+                            V->nvec * sizeof(T), V->nrows, cudaMemcpyHostToDevice, stream()));
+  rt().sync();
+}
+template <class T>
+void mvec_download(Mvec<T>* V)
+{
+  if (V->nrows == 0) return;
+  T* h = V->h();
+  PB_CUDA(cudaMemcpy2DAsync(h, V->lda * sizeof(T), V->d(), V->lda * sizeof(T),
+                            V->nvec * sizeof(T), V->nrows, cudaMemcpyDeviceToHost, stream()));
+  rt().sync();
+}
+
+template <class T>
+void mvec_get_data(const void* vV, T* data, int32_t lda, int row_major)
+{
+  Mvec<T>* V = MV<T>(vV);
+  PB_REQUIRE(data || V->nrows == 0, PB_BAD_CAST, "data is NULL");
+  if (V->nrows == 0) return;
+  if (row_major) {
+    PB_REQUIRE(lda >= V->nvec, PB_INVALID_INPUT, "lda %d < nvec %d", lda, V->nvec);
+    PB_CUDA(cudaMemcpy2DAsync(data, (size_t)lda * sizeof(T), V->d(), V->lda * sizeof(T),
+                              V->nvec * sizeof(T), V->nrows, cudaMemcpyDeviceToHost, stream()));
+    rt().sync();
+  } else {
+    PB_REQUIRE(lda >= V->nrows, PB_INVALID_INPUT, "lda %d < nrows %d", lda, V->nrows);
+    // transpose on the device into scratch, then one 2D copy
+    T* tmp = (T*)rt().scratch(sizeof(T) * (size_t)V->nrows * V->nvec);
+    k_sd_copy<T><<<grid_for((int64_t)V->nrows * V->nvec), 256, 0, stream()>>>(
+        V->d(), V->lda, tmp, V->nrows, V->nrows, V->nvec, 1);
+    PB_LAUNCH_CHECK();
+    PB_CUDA(cudaMemcpy2DAsync(data, (size_t)lda * sizeof(T), tmp, V->nrows * sizeof(T),
+                              V->nrows * sizeof(T), V->nvec, cudaMemcpyDeviceToHost, stream()));
+    rt().sync();
+  }
+}
+
+template <class T>
+void mvec_set_data(void* vV, const T* data, int32_t lda, int row_major)
+{
+  Mvec<T>* V = MV<T>(vV);
+  PB_REQUIRE(data || V->nrows == 0, PB_BAD_CAST, "data is NULL");
+  if (V->nrows == 0) return;
+  if (row_major) {
+    PB_REQUIRE(lda >= V->nvec, PB_INVALID_INPUT, "lda %d < nvec %d", lda, V->nvec);
+    PB_CUDA(cudaMemcpy2DAsync(V->d(), V->lda * sizeof(T), data, (size_t)lda * sizeof(T),
+                              V->nvec * sizeof(T), V->nrows, cudaMemcpyHostToDevice, stream()));
+    rt().sync();
+  } else {
+    PB_REQUIRE(lda >= V->nrows, PB_INVALID_INPUT, "lda %d < nrows %d", lda, V->nrows);
+    T* tmp = (T*)rt().scratch(sizeof(T) * (size_t)V->nrows * V->nvec);
+    PB_CUDA(cudaMemcpy2DAsync(tmp, V->nrows * sizeof(T), data, (size_t)lda * sizeof(T),
+                              V->nrows * sizeof(T), V->nvec, cudaMemcpyHostToDevice, stream()));
+    k_sd_copy<T><<<grid_for((int64_t)V->nrows * V->nvec), 256, 0, stream()>>>(
+        tmp, V->nrows, V->d(), V->lda, V->nvec, V->nrows, 1);
+    PB_LAUNCH_CHECK();
+    rt().sync();
+  }
+}
+
+// ======================================================================
+// sdMat object model
+// ======================================================================
+template <class T>
+void sdmat_create(void** M, int nrows, int ncols, const void* comm)
+{
+  ensure_init();
+  PB_REQUIRE(M, PB_BAD_CAST, "M is NULL");
+  PB_REQUIRE(nrows >= 0 && ncols >= 0, PB_INVALID_INPUT, "negative sdMat size");
+  SdMat<T>* s = new SdMat<T>();
+  s->comm = (const Comm*)comm;
+  s->nrows = nrows;
+  s->ncols = ncols;
+  s->lda = nrows > 0 ? nrows : 1;
+  s->root = s;
+  size_t bytes = sizeof(T) * (size_t)s->lda * (size_t)(ncols > 0 ? ncols : 1);
+  s->d_base = (T*)rt().dmalloc(bytes);
+  s->h_base = (T*)calloc(1, bytes);
+  PB_REQUIRE(s->h_base, PB_MEM_ALLOC_FAILED, "sdMat host allocation failed");
+  PB_CUDA(cudaMemsetAsync(s->d_base, 0, bytes, stream()));
+  *M = s;
+}
+
+template <class T>
+void sdmat_delete(void* vM)
+{
+  if (!vM) return;
+  SdMat<T>* s = (SdMat<T>*)vM;
+  if (!s->is_view()) {
+    rt().dfree(s->d_base);
+    free(s->h_base);
+  }
+  delete s;
+}
+
+template <class T>
+void sd_upload(SdMat<T>* M)
+{
+  if (M->nrows == 0 || M->ncols == 0) return;
+  PB_CUDA(cudaMemcpy2DAsync(M->d(), M->lda * sizeof(T), M->h(), M->lda * sizeof(T),
+                            M->nrows * sizeof(T), M->ncols, cudaMemcpyHostToDevice, stream()));
+  rt().sync();
+}
+template <class T>
+void sd_download(SdMat<T>* M)
+{
+  if (M->nrows == 0 || M->ncols == 0) return;
+  PB_CUDA(cudaMemcpy2DAsync(M->h(), M->lda * sizeof(T), M->d(), M->lda * sizeof(T),
+                            M->nrows * sizeof(T), M->ncols, cudaMemcpyDeviceToHost, stream()));
+  rt().sync();
+}
+
+// after a host-side sdMat operation: upload unless RUN_ON_HOST only
+inline bool sd_host_only(int flags)
+{
+  return (flags & (PB_SDMAT_RUN_ON_HOST | PB_SDMAT_RUN_ON_DEVICE)) == PB_SDMAT_RUN_ON_HOST;
+}
+// after a device-side sdMat result: download unless RUN_ON_DEVICE only
+inline bool sd_device_only(int flags)
+{
+  return (flags & (PB_SDMAT_RUN_ON_HOST | PB_SDMAT_RUN_ON_DEVICE)) == PB_SDMAT_RUN_ON_DEVICE;
+}
+
+template <class T>
+inline T& sdh(SdMat<T>* M, int i, int j)
+{
+  return M->h()[i + (int64_t)j * M->lda];
+}
+
+template <class T>
+void sdmat_view_block(void* vM, void** vblock, int imin, int imax, int jmin, int jmax)
+{
+  SdMat<T>* M = SD<T>(vM);
+  PB_REQUIRE(vblock, PB_BAD_CAST, "Mblock is NULL");
+  PB_REQUIRE(imin >= 0 && imax < M->nrows && jmin >= 0 && jmax < M->ncols && imin <= imax + 1 &&
+                 jmin <= jmax + 1,
+             PB_INVALID_INPUT, "sdMat view (%d:%d,%d:%d) out of range %dx%d", imin, imax, jmin,
+             jmax, M->nrows, M->ncols);
+  SdMat<T>* b = (SdMat<T>*)*vblock;
+  if (b && !b->is_view()) {
+    sdmat_delete<T>(b);
+    b = nullptr;
+  }
+  if (!b) b = new SdMat<T>();
+  b->comm = M->comm;
+  b->nrows = imax - imin + 1;
+  b->ncols = jmax - jmin + 1;
+  b->lda = M->lda;
+  b->root = M->root;
+  b->row_off = M->row_off + imin;
+  b->col_off = M->col_off + jmin;
+  *vblock = b;
+}
+
+// ======================================================================
+// sparse matrix construction (host CRS -> SELL-C-sigma in HBM)
+// ======================================================================
+template <class T>
+void sell_free(SparseMat<T>* A)
+{
+  rt().dfree(A->d_chunk_ptr);
+  rt().dfree(A->d_chunk_len);
+  rt().dfree(A->d_col);
+  rt().dfree(A->d_val);
+  rt().dfree(A->d_perm);
+  rt().dfree(A->d_row_len);
+  rt().dfree(A->d_diag);
+}
+
+template <class T>
+void* upload_vec(const std::vector<T>& v)
+{
+  if (v.empty()) return nullptr;
+  void* d = rt().dmalloc(v.size() * sizeof(T));
+  PB_CUDA(cudaMemcpyAsync(d, v.data(), v.size() * sizeof(T), cudaMemcpyHostToDevice, stream()));
+  return d;
+}
+
+// rows stably sorted by column inside each row (the builtin's
+// sort_global_cols, crsmat_module.F90:484-516), then laid out as SELL-C-sigma
+template <class T>
+SparseMat<T>* build_sparse(const Comm* comm, int64_t nrows, int64_t ncols,
+                           std::vector<int64_t>&& rp, std::vector<int32_t>&& col,
+                           std::vector<T>&& val, int flags)
+{
+  ensure_init();
+  PB_REQUIRE(nrows >= 0 && nrows < (int64_t(1) << 31) && ncols >= 0 && ncols < (int64_t(1) << 31),
+             PB_INTEGER_OVERFLOW, "matrix dimensions %lld x %lld exceed 32-bit local indices",
+             (long long)nrows, (long long)ncols);
+  const int64_t nnz = rp[nrows];
+  // sort columns inside rows (stable)
+  {
+    std::vector<int64_t> idx;
+    std::vector<int32_t> c2;
+    std::vector<T> v2;
+    for (int64_t i = 0; i < nrows; i++) {
+      const int64_t p0 = rp[i], p1 = rp[i + 1], len = p1 - p0;
+      bool sorted = true;
+      for (int64_t p = p0 + 1; p < p1; p++)
+        if (col[p] < col[p - 1]) { sorted = false; break; }
+      if (sorted) continue;
+      idx.resize(len);
+      std::iota(idx.begin(), idx.end(), p0);
+      std::stable_sort(idx.begin(), idx.end(), [&](int64_t a, int64_t b) { return col[a] < col[b]; });
+      c2.resize(len);
+      v2.resize(len);
+      for (int64_t q = 0; q < len; q++) { c2[q] = col[idx[q]]; v2[q] = val[idx[q]]; }
+      for (int64_t q = 0; q < len; q++) { col[p0 + q] = c2[q]; val[p0 + q] = v2[q]; }
+    }
+  }
+  for (int64_t p = 0; p < nnz; p++)
+    PB_REQUIRE(col[p] >= 0 && col[p] < ncols, PB_INVALID_INPUT,
+               "column index %d out of range [0,%lld)", col[p], (long long)ncols);
+
+  SparseMat<T>* A = new SparseMat<T>();
+  A->comm = comm;
+  A->nrows = nrows;
+  A->ncols = ncols;
+  A->nnz = nnz;
+  A->C = rt().sell_C;
+  A->sigma = (flags & (PB_SPARSEMAT_PERM_LOCAL | PB_SPARSEMAT_PERM_GLOBAL)) ? rt().sell_sigma_default : 1;
+  if (A->sigma < 1) A->sigma = 1;
+  const int C = A->C;
+
+  // sigma permutation: stable descending row length inside windows
+  std::vector<int32_t> perm(nrows);
+  std::iota(perm.begin(), perm.end(), 0);
+  if (A->sigma > 1) {
+    for (int64_t w0 = 0; w0 < nrows; w0 += A->sigma) {
+      const int64_t w1 = std::min(nrows, w0 + A->sigma);
+      std::stable_sort(perm.begin() + w0, perm.begin() + w1, [&](int32_t a, int32_t b) {
+        return (rp[a + 1] - rp[a]) > (rp[b + 1] - rp[b]);
+      });
+    }
+  }
+  bool ident = true;
+  for (int64_t r = 0; r < nrows; r++)
+    if (perm[r] != r) { ident = false; break; }
+
+  A->nchunks = ceil_div(nrows, C);
+  std::vector<int32_t> clen(A->nchunks, 0);
+  std::vector<int64_t> cptr(A->nchunks + 1, 0);
+  std::vector<int32_t> rlen(A->nchunks * C, 0);
+  int maxlen = 0;
+  for (int64_t r = 0; r < nrows; r++) {
+    const int len = (int)(rp[perm[r] + 1] - rp[perm[r]]);
+    rlen[r] = len;
+    clen[r / C] = std::max(clen[r / C], len);
+    maxlen = std::max(maxlen, len);
+  }
+  for (int64_t c = 0; c < A->nchunks; c++) cptr[c + 1] = cptr[c] + (int64_t)clen[c] * C;
+  A->nnz_padded = cptr[A->nchunks];
+  A->max_row_len = maxlen;
+  std::vector<int32_t> scol(A->nnz_padded > 0 ? A->nnz_padded : 1, 0);
+  std::vector<T> sval(A->nnz_padded > 0 ? A->nnz_padded : 1, T(0));
+  for (int64_t r = 0; r < A->nchunks * C; r++) {
+    const int64_t ch = r / C, l = r - ch * C;
+    const int64_t base = cptr[ch] + l;
+    if (r < nrows) {
+      const int64_t i = perm[r];
+      const int64_t p0 = rp[i];
+      const int len = rlen[r];
+      const int32_t padc = len > 0 ? col[p0] : 0;
+      for (int k = 0; k < clen[ch]; k++) {
+        if (k < len) {
+          scol[base + (int64_t)k * C] = col[p0 + k];
+          sval[base + (int64_t)k * C] = val[p0 + k];
+        } else {
+          scol[base + (int64_t)k * C] = padc;
+        }
+      }
+    }
+  }
+  std::vector<T> diag(nrows, T(0));
+  for (int64_t i = 0; i < nrows; i++)
+    for (int64_t p = rp[i]; p < rp[i + 1]; p++)
+      if (col[p] == i) diag[i] = val[p];
+
+  A->d_chunk_ptr = (int64_t*)upload_vec(cptr);
+  A->d_chunk_len = (int32_t*)upload_vec(clen);
+  A->d_col = (int32_t*)upload_vec(scol);
+  A->d_val = (T*)upload_vec(sval);
+  A->d_perm = ident ? nullptr : (int32_t*)upload_vec(perm);
+  A->d_row_len = (int32_t*)upload_vec(rlen);
+  A->d_diag = (T*)upload_vec(diag);
+  rt().sync();
+
+  A->row_map = new Map();
+  A->row_map->comm = comm;
+  A->row_map->nglob = nrows;
+  A->row_map->nloc = (int32_t)nrows;
+  if (ncols == nrows) {
+    A->dom_map = A->row_map;
+  } else {
+    A->dom_map = new Map();
+    A->dom_map->comm = comm;
+    A->dom_map->nglob = ncols;
+    A->dom_map->nloc = (int32_t)ncols;
+  }
+  A->ctx = new Context();
+  A->ctx->row_map = A->row_map;
+  A->ctx->col_map = A->dom_map;
+  A->ctx->range_map = A->row_map;
+  A->ctx->domain_map = A->dom_map;
+  A->h_row_ptr = std::move(rp);
+  A->h_col = std::move(col);
+  A->h_val = std::move(val);
+  A->h_perm = std::move(perm);
+  return A;
+}
+
+template <class T>
+void sparse_delete(void* vA)
+{
+  if (!vA) return;
+  SparseMat<T>* A = (SparseMat<T>*)vA;
+  sell_free(A);
+  if (A->dom_map != A->row_map) delete A->dom_map;
+  delete A->row_map;
+  delete A->ctx;
+  delete A;
+}
+
+typedef int (*RowFunc)(int64_t, int32_t*, int64_t*, void*, void*);
+typedef int (*RowFuncCtor)(void*, void**);
+
+template <class T>
+void create_from_rowfunc(void** vA, const void* comm, int64_t nrows, int64_t ncols, int32_t maxnne,
+                         RowFunc f, RowFuncCtor ctor, void* arg, int flags)
+{
+  PB_REQUIRE(vA && comm && f, PB_BAD_CAST, "NULL argument");
+  PB_REQUIRE(maxnne >= 0, PB_INVALID_INPUT, "maxnne < 0");
+  std::vector<int64_t> rp(nrows + 1, 0);
+  std::vector<int32_t> col;
+  std::vector<T> val;
+  col.reserve((size_t)nrows * (maxnne > 0 ? maxnne : 1));
+  val.reserve((size_t)nrows * (maxnne > 0 ? maxnne : 1));
+  std::vector<int64_t> cbuf(maxnne > 0 ? maxnne : 1);
+  std::vector<T> vbuf(maxnne > 0 ? maxnne : 1);
+  void* work = arg;
+  if (ctor) {
+    work = nullptr;
+    PB_REQUIRE(ctor(arg, &work) == 0, PB_FUNCTIONAL_ERROR, "row function constructor failed");
+  }
+  for (int64_t i = 0; i < nrows; i++) {
+    int32_t len = 0;
+    int err = f(i, &len, cbuf.data(), vbuf.data(), work);
+    PB_REQUIRE(err == 0, PB_FUNCTIONAL_ERROR, "row function returned %d for row %lld", err,
+               (long long)i);
+    PB_REQUIRE(len >= 0 && len <= maxnne, PB_INVALID_INPUT, "row %lld has %d > maxnne=%d entries",
+               (long long)i, len, maxnne);
+    for (int q = 0; q < len; q++) {
+      col.push_back((int32_t)cbuf[q]);
+      val.push_back(vbuf[q]);
+    }
+    rp[i + 1] = (int64_t)col.size();
+  }
+  if (ctor) ctor(arg, &work);
+  *vA = build_sparse<T>((const Comm*)comm, nrows, ncols, std::move(rp), std::move(col),
+                        std::move(val), flags);
+}
+
+template <class T>
+void read_mm(void** vA, const void* comm, const char* fn, int flags)
+{
+  PB_REQUIRE(vA && fn, PB_BAD_CAST, "NULL argument");
+  FILE* f = fopen(fn, "r");
+  PB_REQUIRE(f, PB_INVALID_INPUT, "cannot open %s", fn);
+  char line[1024];
+  bool symmetric = false, skew = false, pattern = false;
+  if (!fgets(line, sizeof line, f)) { fclose(f); PB_THROW(PB_INVALID_INPUT, "empty file %s", fn); }
+  std::string hdr(line);
+  for (auto& ch : hdr) ch = (char)tolower(ch);
+  if (hdr.find("complex") != std::string::npos) { fclose(f); PB_THROW(PB_NOT_IMPLEMENTED, "complex MatrixMarket not supported"); }
+  symmetric = hdr.find("symmetric") != std::string::npos && hdr.find("skew") == std::string::npos;
+  skew = hdr.find("skew-symmetric") != std::string::npos;
+  pattern = hdr.find("pattern") != std::string::npos;
+  do {
+    if (!fgets(line, sizeof line, f)) { fclose(f); PB_THROW(PB_INVALID_INPUT, "truncated %s", fn); }
+  } while (line[0] == '%');
+  long long nr, nc, nz;
+  PB_REQUIRE(sscanf(line, "%lld %lld %lld", &nr, &nc, &nz) == 3, PB_INVALID_INPUT, "bad size line");
+  std::vector<int64_t> ri, ci;
+  std::vector<T> vv;
+  for (long long q = 0; q < nz; q++) {
+    long long i, j;
+    double v = 1.0;
+    if (!fgets(line, sizeof line, f)) break;
+    int got = pattern ? sscanf(line, "%lld %lld", &i, &j) : sscanf(line, "%lld %lld %lf", &i, &j, &v);
+    if (got < 2) { q--; continue; }
+    ri.push_back(i - 1); ci.push_back(j - 1); vv.push_back(T(v));
+    if ((symmetric || skew) && i != j) {
+      ri.push_back(j - 1); ci.push_back(i - 1); vv.push_back(T(skew ? -v : v));
+    }
+  }
+  fclose(f);
+  std::vector<int64_t> rp(nr + 1, 0);
+  for (auto r : ri) rp[r + 1]++;
+  for (long long r = 0; r < nr; r++) rp[r + 1] += rp[r];
+  std::vector<int32_t> col(ri.size());
+  std::vector<T> val(ri.size());
+  std::vector<int64_t> fill(rp.begin(), rp.end() - 1);
+  for (size_t q = 0; q < ri.size(); q++) {  // file order kept inside a row
+    const int64_t p = fill[ri[q]]++;
+    col[p] = (int32_t)ci[q];
+    val[p] = vv[q];
+  }
+  *vA = build_sparse<T>((const Comm*)comm, nr, nc, std::move(rp), std::move(col), std::move(val), flags);
+}
+
+// ======================================================================
+// SpMMV launches
+// ======================================================================
+template <class T>
+SellDev<T> sell_dev(const SparseMat<T>* A)
+{
+  SellDev<T> s;
+  s.nrows = A->nrows;
+  s.nchunks = A->nchunks;
+  s.C = A->C;
+  s.chunk_ptr = A->d_chunk_ptr;
+  s.chunk_len = A->d_chunk_len;
+  s.col = A->d_col;
+  s.val = A->d_val;
+  s.perm = A->d_perm;
+  return s;
+}
+
+struct SpmvOut {
+  bool wdw = false, vdw = false;
+};
+
+template <class T, int NV, int TPR>
+void launch_spmv_nv(const SellDev<T>& S, SpmvArgs<T>& p, int64_t nrows_padded, bool vec)
+{
+  constexpr int RPB = SPMV_BS / TPR;
+  const int grid = (int)ceil_div(nrows_padded > 0 ? nrows_padded : 1, RPB);
+  if (p.want_wdw || p.want_vdw) {
+    p.part = (T*)rt().scratch(sizeof(T) * (size_t)grid * 2 * NV);
+    p.counter = rt().counters();
+  }
+  if (vec)
+    k_sell_spmmv<T, NV, TPR, true><<<grid, SPMV_BS, 0, stream()>>>(S, p);
+  else
+    k_sell_spmmv<T, NV, TPR, false><<<grid, SPMV_BS, 0, stream()>>>(S, p);
+  PB_LAUNCH_CHECK();
+}
+
+template <class T>
+bool aligned16(const void* p)
+{
+  return ((uintptr_t)p & 15u) == 0;
+}
+
+// Y(:,col0:col0+nv) = alpha*(A+diag(sh))X + beta*Y, nv <= 32, epilogues on
+template <class T>
+void spmv_tile(const SparseMat<T>* A, SpmvArgs<T>& p, int nv)
+{
+  const SellDev<T> S = sell_dev(A);
+  const int64_t npad = A->nchunks * (int64_t)A->C;
+  p.nvec = nv;
+  int NV = nv <= 1 ? 1 : nv <= 2 ? 2 : nv <= 4 ? 4 : nv <= 8 ? 8 : nv <= 16 ? 16 : 32;
+  // vector path: the tile width is exactly NV and every row segment that a
+  // thread touches starts on a 16-byte boundary
+  const int vw = 16 / (int)sizeof(T);
+  bool vec = (nv == NV) && NV >= 2;
+  if (vec) {
+    vec = aligned16<T>(p.x + p.col0) && aligned16<T>(p.y + p.col0) && (p.ldx % vw == 0) &&
+          (p.ldy % vw == 0) && (!p.u || (aligned16<T>(p.u + p.col0) && p.ldu % vw == 0));
+    if (sizeof(T) == 4 && NV == 2) vec = false;
+  }
+  if (sizeof(T) == 8) {
+    switch (NV) {
+      case 1: launch_spmv_nv<T, 1, 1>(S, p, npad, false); break;
+      case 2: launch_spmv_nv<T, 2, 1>(S, p, npad, vec); break;
+      case 4: launch_spmv_nv<T, 4, 1>(S, p, npad, vec); break;
+      case 8: launch_spmv_nv<T, 8, 2>(S, p, npad, vec); break;
+      case 16: launch_spmv_nv<T, 16, 4>(S, p, npad, vec); break;
+      default: launch_spmv_nv<T, 32, 8>(S, p, npad, vec); break;
+    }
+  } else {
+    switch (NV) {
+      case 1: launch_spmv_nv<T, 1, 1>(S, p, npad, false); break;
+      case 2: launch_spmv_nv<T, 2, 1>(S, p, npad, false); break;
+      case 4: launch_spmv_nv<T, 4, 1>(S, p, npad, vec); break;
+      case 8: launch_spmv_nv<T, 8, 2>(S, p, npad, vec); break;
+      case 16: launch_spmv_nv<T, 16, 4>(S, p, npad, vec); break;
+      default: launch_spmv_nv<T, 32, 8>(S, p, npad, vec); break;
+    }
+  }
+}
+
+// general entry: tiles of <= 32 columns; dots returned to host arrays
+template <class T>
+void spmv_general(T alpha, const SparseMat<T>* A, const T* shifts, const Mvec<T>* X, T beta,
+                  Mvec<T>* Y, T* WdotW, T* VdotW, T gamma, T delta, Mvec<T>* U)
+{
+  PB_REQUIRE(X->nvec == Y->nvec, PB_INVALID_INPUT, "X has %d columns, Y %d", X->nvec, Y->nvec);
+  PB_REQUIRE(X->nrows == A->ncols && Y->nrows == A->nrows, PB_INVALID_INPUT,
+             "shape mismatch: A %lldx%lld, X %d rows, Y %d rows", (long long)A->nrows,
+             (long long)A->ncols, X->nrows, Y->nrows);
+  if (U) {
+    PB_REQUIRE(U->nvec == Y->nvec && U->nrows == Y->nrows, PB_INVALID_INPUT, "U shape mismatch");
+  }
+  const int nvec = X->nvec;
+  if (alpha == T(0) || A->nnz == 0) {
+    // crsmat_module.F90:1508-1511: only scale Y; the fused extras still apply
+    if (Y->nrows > 0) {
+      k_scale_rows<T><<<grid_for((int64_t)Y->nrows * nvec), 256, 0, stream()>>>(Y->d(), Y->lda, Y->nrows, nvec, beta);
+      PB_LAUNCH_CHECK();
+    }
+    if (!WdotW && !VdotW && !U) return;
+    // fall through with alpha = 0: the kernel computes y = beta*y once more
+    // from the scaled values would be wrong, so do the extras explicitly
+    if (U) {
+      k_axpby<T><<<grid_for((int64_t)Y->nrows * nvec), 256, 0, stream()>>>(Y->d(), Y->lda, U->d(), U->lda, Y->nrows, nvec, gamma, nullptr, delta);
+      PB_LAUNCH_CHECK();
+    }
+    T* dd = (T*)rt().dmalloc(sizeof(T) * 64);
+    for (int c0 = 0; c0 < nvec; c0 += 64) {
+      const int nv = std::min(64, nvec - c0);
+      auto dotk = [&](const Mvec<T>* P, int poff, T* out) {
+        const int grid = std::min(grid_for(P->nrows), rt().num_sms() * 4);
+        T* part = (T*)rt().scratch(sizeof(T) * (size_t)grid * 64);
+        k_coldot<T, 64><<<grid, 256, 0, stream()>>>(P->d() + poff, P->lda, Y->d() + c0, Y->lda, Y->nrows, nv, part, rt().counters(), dd);
+        PB_LAUNCH_CHECK();
+        std::vector<T> h(64);
+        PB_CUDA(cudaMemcpyAsync(h.data(), dd, sizeof(T) * 64, cudaMemcpyDeviceToHost, stream()));
+        rt().sync();
+        for (int j = 0; j < nv; j++) out[c0 + j] = h[j];
+      };
+      if (WdotW) dotk(Y, c0, WdotW);
+      if (VdotW) dotk(X, c0, VdotW);
+    }
+    rt().dfree(dd);
+    return;
+  }
+  T* dots_dev = nullptr;
+  std::vector<T> hd;
+  if (WdotW || VdotW) {
+    dots_dev = (T*)rt().dmalloc(sizeof(T) * 64);
+    hd.resize(64);
+  }
+  for (int c0 = 0; c0 < nvec; c0 += 32) {
+    const int nv = std::min(32, nvec - c0);
+    SpmvArgs<T> p;
+    memset(&p, 0, sizeof(p));
+    p.alpha = alpha;
+    p.beta = beta;
+    p.x = X->d();
+    p.ldx = X->lda;
+    p.y = Y->d();
+    p.ldy = Y->lda;
+    p.col0 = c0;
+    p.want_wdw = WdotW != nullptr;
+    p.want_vdw = VdotW != nullptr;
+    p.dots_out = dots_dev;
+    p.gamma = gamma;
+    p.delta = delta;
+    p.u = U ? U->d() : nullptr;
+    p.ldu = U ? U->lda : 0;
+    if (shifts) {
+      p.has_shift = 1;
+      for (int j = 0; j < nv; j++) p.sh[j] = shifts[c0 + j];
+    }
+    spmv_tile<T>(A, p, nv);
+    if (dots_dev) {
+      const int NV = nv <= 1 ? 1 : nv <= 2 ? 2 : nv <= 4 ? 4 : nv <= 8 ? 8 : nv <= 16 ? 16 : 32;
+      PB_CUDA(cudaMemcpyAsync(hd.data(), dots_dev, sizeof(T) * 2 * NV, cudaMemcpyDeviceToHost, stream()));
+      rt().sync();
+      for (int j = 0; j < nv; j++) {
+        if (WdotW) WdotW[c0 + j] = hd[j];
+        if (VdotW) VdotW[c0 + j] = hd[NV + j];
+      }
+    }
+  }
+  if (dots_dev) rt().dfree(dots_dev);
+}
+
+// ======================================================================
+// block products
+// ======================================================================
+template <class T>
+void launch_mvTmv(int64_t n, int m, int k, T alpha, const T* V, int64_t ldv, const T* W,
+                  int64_t ldw, T beta, T* Cd, int64_t ldc)
+{
+  MvTmvArgs<T> a;
+  a.n = n; a.m = m; a.k = k; a.V = V; a.ldv = ldv; a.W = W; a.ldw = ldw;
+  a.alpha = alpha; a.beta = beta; a.Cd = Cd; a.ldc = ldc;
+  const bool big = (int64_t)m * k >= 256;
+  const int TM = big ? 8 : 4, TK = big ? 8 : 4;
+  const int mp = ceil_div(m, TM) * TM, kp = ceil_div(k, TK) * TK;
+  const int nt = (mp / TM) * (kp / TK);
+  PB_REQUIRE(nt <= BLK_BS, PB_NOT_IMPLEMENTED, "mvecT_times_mvec with %dx%d result exceeds one block's tiles", m, k);
+  const int RG = BLK_BS / nt;
+  a.R = std::max(32, ((RG * 4 + 31) / 32) * 32);
+  a.R = std::min(a.R, 128);
+  size_t smem = sizeof(T) * (size_t)a.R * (mp + kp);
+  const size_t red = sizeof(T) * (size_t)RG * mp * kp;
+  if (red > smem) smem = red;
+  const int64_t ntiles = ceil_div(n > 0 ? n : 1, a.R);
+  const int grid = (int)std::min<int64_t>(ntiles, (int64_t)rt().num_sms() * 2);
+  a.part = (T*)rt().scratch(sizeof(T) * (size_t)grid * m * k);
+  a.counter = rt().counters();
+  if (big) {
+    auto kern = k_mvTmv<T, 8, 8>;
+    PB_CUDA(cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+    kern<<<grid, BLK_BS, smem, stream()>>>(a);
+  } else {
+    auto kern = k_mvTmv<T, 4, 4>;
+    PB_CUDA(cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+    kern<<<grid, BLK_BS, smem, stream()>>>(a);
+  }
+  PB_LAUNCH_CHECK();
+}
+
+template <class T>
+void launch_rowgemm(RowGemmArgs<T>& a)
+{
+  // micro-tile: TK columns per thread, TR rows
+  const int TK = a.k >= 32 ? 8 : a.k >= 8 ? 4 : a.k >= 2 ? 2 : 1;
+  const int kp = ceil_div(a.k, TK) * TK;
+  const int ntk = kp / TK;
+  const int ntr = BLK_BS / ntk;
+  const int TR = (a.k >= 32) ? 4 : 1;
+  a.R = ntr * TR;
+  const int ap = a.m + (a.m & 1);
+  const int mvp = a.mv + (a.mv & 1);
+  size_t smem = sizeof(T) * ((size_t)a.R * ap + (size_t)a.R * kp + (size_t)ap * kp +
+                             (a.mode == RM_VCWD ? (size_t)kp * kp : 0) +
+                             (a.gram == GM_VW ? (size_t)a.R * mvp : 0));
+  PB_REQUIRE(smem <= 227 * 1024, PB_NOT_IMPLEMENTED, "block product too wide for one tile (%zu bytes of shared memory)", smem);
+  const int gm = (a.gram == GM_WW) ? a.k : a.mv;
+  PB_REQUIRE(a.gram == GM_NONE || gm * a.k <= 16 * BLK_BS, PB_NOT_IMPLEMENTED, "fused Gram matrix larger than 64x64");
+  const int64_t ntiles = ceil_div(a.n > 0 ? a.n : 1, a.R);
+  const int grid = (int)std::min<int64_t>(ntiles, (int64_t)rt().num_sms() * 4);
+  if (a.gram != GM_NONE) {
+    a.part = (T*)rt().scratch(sizeof(T) * (size_t)grid * gm * a.k);
+    a.counter = rt().counters();
+  }
+#define PB_RG_LAUNCH(TRv, TKv)                                                                 \
+  {                                                                                            \
+    auto kern = k_rowgemm<T, TRv, TKv>;                                                        \
+    PB_CUDA(cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem)); \
+    kern<<<grid, BLK_BS, smem, stream()>>>(a);                                                 \
+  }
+  if (TK == 8) PB_RG_LAUNCH(4, 8)
+  else if (TK == 4) PB_RG_LAUNCH(1, 4)
+  else if (TK == 2) PB_RG_LAUNCH(1, 2)
+  else PB_RG_LAUNCH(1, 1)
+#undef PB_RG_LAUNCH
+  PB_LAUNCH_CHECK();
+}
+
+template <class T>
+RowGemmArgs<T> rowgemm_args()
+{
+  RowGemmArgs<T> a;
+  memset(&a, 0, sizeof(a));
+  a.alpha = T(1);
+  a.galpha = T(1);
+  return a;
+}
+
+// ======================================================================
+// CARP
+// ======================================================================
+template <class T>
+CarpWork<T>* carp_build(const SparseMat<T>* A, int nshifts, const T* sr, const T* si)
+{
+  PB_REQUIRE(A->nrows == A->ncols, PB_INVALID_INPUT, "CARP needs a square matrix");
+  CarpWork<T>* w = new CarpWork<T>();
+  w->nshifts = nshifts;
+  w->sigma_r.assign(sr, sr + nshifts);
+  if (si) w->sigma_i.assign(si, si + nshifts);
+  else w->sigma_i.assign(nshifts, T(0));
+  const int64_t n = A->nrows;
+  std::vector<int32_t> color;
+  w->ncolors = dist2_color(n, A->ncols, A->h_row_ptr, A->h_col, color);
+  w->h_color_ptr.assign(w->ncolors + 1, 0);
+  for (int64_t i = 0; i < n; i++) w->h_color_ptr[color[i] + 1]++;
+  for (int c = 0; c < w->ncolors; c++) w->h_color_ptr[c + 1] += w->h_color_ptr[c];
+  std::vector<int32_t> rows(n);
+  {
+    std::vector<int64_t> fill(w->h_color_ptr.begin(), w->h_color_ptr.end() - 1);
+    for (int64_t i = 0; i < n; i++) rows[fill[color[i]]++] = (int32_t)i;
+  }
+  std::vector<int64_t> rp(n + 1, 0);
+  std::vector<int32_t> col;
+  std::vector<T> val, nrm(n), dg(n);
+  col.reserve(A->nnz);
+  val.reserve(A->nnz);
+  for (int64_t q = 0; q < n; q++) {
+    const int64_t i = rows[q];
+    T s = T(0), d = T(0);
+    for (int64_t p = A->h_row_ptr[i]; p < A->h_row_ptr[i + 1]; p++) {
+      col.push_back(A->h_col[p]);
+      val.push_back(A->h_val[p]);
+      s += A->h_val[p] * A->h_val[p];
+      if (A->h_col[p] == i) d = A->h_val[p];
+    }
+    nrm[q] = s;
+    dg[q] = d;
+    rp[q + 1] = (int64_t)col.size();
+  }
+  w->nrows = n;
+  w->d_rows = (int32_t*)upload_vec(rows);
+  w->d_rp = (int64_t*)upload_vec(rp);
+  w->d_col = (int32_t*)upload_vec(col);
+  w->d_val = (T*)upload_vec(val);
+  w->d_nrm = (T*)upload_vec(nrm);
+  w->d_diag = (T*)upload_vec(dg);
+  rt().sync();
+  return w;
+}
+
+template <class T>
+void carp_free(CarpWork<T>* w)
+{
+  if (!w) return;
+  rt().dfree(w->d_rows);
+  rt().dfree(w->d_rp);
+  rt().dfree(w->d_col);
+  rt().dfree(w->d_val);
+  rt().dfree(w->d_nrm);
+  rt().dfree(w->d_diag);
+  delete w;
+}
+
+template <class T, bool RC>
+void carp_run(const CarpWork<T>* w, int nvec, const T* sr, const T* si, const Mvec<T>* B,
+              Mvec<T>* Xr, Mvec<T>* Xi, const T* omega)
+{
+  for (int c0 = 0; c0 < nvec; c0 += 32) {
+    const int nv = std::min(32, nvec - c0);
+    KaczArgs<T> a;
+    memset(&a, 0, sizeof(a));
+    a.rows = w->d_rows; a.rp = w->d_rp; a.col = w->d_col; a.val = w->d_val;
+    a.nrm = w->d_nrm; a.diag = w->d_diag;
+    a.nvec = nv;
+    for (int j = 0; j < nv; j++) {
+      a.sig_r[j] = sr[c0 + j];
+      a.sig_i[j] = si ? si[c0 + j] : T(0);
+      a.omega[j] = omega[c0 + j];
+    }
+    a.b = B ? B->d() + c0 : nullptr;
+    a.ldb = B ? B->lda : 0;
+    a.xr = Xr->d() + c0;
+    a.ldxr = Xr->lda;
+    a.xi = Xi ? Xi->d() + c0 : nullptr;
+    a.ldxi = Xi ? Xi->lda : 0;
+    auto one = [&](int color) {
+      a.q0 = w->h_color_ptr[color];
+      a.q1 = w->h_color_ptr[color + 1];
+      const int64_t cnt = a.q1 - a.q0;
+      if (cnt <= 0) return;
+      const int grid = (int)ceil_div(cnt, 256);
+#define PB_KZ(NVv)                                                       \
+  k_kacz_color<T, NVv, RC><<<grid, 256, 0, stream()>>>(a);
+      if (nv <= 1) PB_KZ(1)
+      else if (nv <= 2) PB_KZ(2)
+      else if (nv <= 4) PB_KZ(4)
+      else if (nv <= 8) PB_KZ(8)
+      else if (nv <= 16) PB_KZ(16)
+      else PB_KZ(32)
+#undef PB_KZ
+      PB_LAUNCH_CHECK();
+    };
+    for (int c = 0; c < w->ncolors; c++) one(c);        // forward
+    for (int c = w->ncolors - 1; c >= 0; c--) one(c);   // backward
+  }
+}
+
+}  // namespace pb

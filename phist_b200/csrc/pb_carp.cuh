@@ -1,0 +1,156 @@
+// pb_carp.cuh -- CARP: Kaczmarz forward/backward sweeps on (A - sigma_j I)
+// (carp_setup/carp_sweep/carp_destroy, phist_kernels_carp_decl.h:35-106).
+//
+// The builtin sweep is row-sequential (kacz_loop_seq_def.h) or runs over the
+// rows of a distance-2 colouring (kacz_loop_clr_def.h).  On the GPU every
+// colour class is one launch: rows of one colour share no column, so their
+// projections touch disjoint entries of X and may run concurrently; the
+// result equals the sequential sweep over the rows in colour order.  The
+// update formulae are those of kacz_sub_def.h:50-150:
+//   tmp_j  = sum_k a_ik x_kj - sigma_j x_ij - b_ij
+//   rn_j   = sum_k a_ik^2 - 2 a_ii sigma_j + sigma_j^2   (1 if zero)
+//   tmp_j *= omega_j / rn_j
+//   x_ij  += tmp_j sigma_j ;  x_kj -= tmp_j a_ik  for every entry k of row i
+// The matrix is stored once more in colour order (CRS), so the rows of one
+// launch are contiguous and their entries are read with coalesced loads.
+#pragma once
+#include "pb_core.hpp"
+
+namespace pb {
+
+template <class T>
+struct CarpWork {
+  int nshifts = 0;
+  std::vector<T> sigma_r, sigma_i;
+  int ncolors = 0;
+  std::vector<int64_t> h_color_ptr;  // rows [color_ptr[c], color_ptr[c+1]) of the colour order
+  int32_t* d_rows = nullptr;         // colour order -> original row
+  int64_t* d_rp = nullptr;           // CRS in colour order
+  int32_t* d_col = nullptr;
+  T* d_val = nullptr;
+  T* d_nrm = nullptr;                // sum_k a_ik^2 per colour-ordered row
+  T* d_diag = nullptr;               // a_ii per colour-ordered row
+  int64_t nrows = 0;
+};
+
+template <class T>
+struct KaczArgs {
+  const int32_t* __restrict__ rows;
+  const int64_t* __restrict__ rp;
+  const int32_t* __restrict__ col;
+  const T* __restrict__ val;
+  const T* __restrict__ nrm;
+  const T* __restrict__ diag;
+  int64_t q0, q1;       // colour-ordered row range of this launch
+  int nvec;
+  T sig_r[32];
+  T sig_i[32];
+  T omega[32];
+  const T* b; int64_t ldb;   // may be nullptr (b = 0)
+  T* xr; int64_t ldxr;
+  T* xi; int64_t ldxi;       // rc variant only
+};
+
+// one thread per row, NV columns masked to nvec
+template <class T, int NV, bool RC>
+__global__ void __launch_bounds__(256) k_kacz_color(KaczArgs<T> a)
+{
+  const int64_t q = a.q0 + blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
+  if (q >= a.q1) return;
+  const int64_t i = a.rows[q];
+  const int64_t p0 = a.rp[q], p1 = a.rp[q + 1];
+  T tr[NV], ti[NV];
+#pragma unroll
+  for (int j = 0; j < NV; j++) {
+    tr[j] = T(0);
+    ti[j] = T(0);
+    if (j < a.nvec) {
+      const T xr = a.xr[i * a.ldxr + j];
+      if (RC) {
+        const T xi = a.xi[i * a.ldxi + j];
+        tr[j] = -a.sig_r[j] * xr + a.sig_i[j] * xi;
+        ti[j] = -a.sig_i[j] * xr - a.sig_r[j] * xi;
+      } else {
+        tr[j] = -a.sig_r[j] * xr;
+      }
+    }
+  }
+  for (int64_t p = p0; p < p1; p++) {
+    const T v = a.val[p];
+    const int64_t c = a.col[p];
+#pragma unroll
+    for (int j = 0; j < NV; j++)
+      if (j < a.nvec) {
+        tr[j] += v * a.xr[c * a.ldxr + j];
+        if (RC) ti[j] += v * a.xi[c * a.ldxi + j];
+      }
+  }
+  const T nrm = a.nrm[q], d = a.diag[q];
+#pragma unroll
+  for (int j = 0; j < NV; j++)
+    if (j < a.nvec) {
+      if (a.b) tr[j] -= a.b[i * a.ldb + j];
+      T rn = nrm - T(2) * d * a.sig_r[j] + a.sig_r[j] * a.sig_r[j];
+      if (RC) rn += a.sig_i[j] * a.sig_i[j];
+      if (rn == T(0)) rn = T(1);
+      const T f = a.omega[j] / rn;
+      tr[j] *= f;
+      if (RC) {
+        ti[j] *= f;
+        a.xr[i * a.ldxr + j] += tr[j] * a.sig_r[j] + ti[j] * a.sig_i[j];
+        a.xi[i * a.ldxi + j] += ti[j] * a.sig_r[j] - tr[j] * a.sig_i[j];
+      } else {
+        a.xr[i * a.ldxr + j] += tr[j] * a.sig_r[j];
+      }
+    }
+  for (int64_t p = p0; p < p1; p++) {
+    const T v = a.val[p];
+    const int64_t c = a.col[p];
+#pragma unroll
+    for (int j = 0; j < NV; j++)
+      if (j < a.nvec) {
+        a.xr[c * a.ldxr + j] -= tr[j] * v;
+        if (RC) a.xi[c * a.ldxi + j] -= ti[j] * v;
+      }
+  }
+}
+
+// Greedy distance-2 colouring in natural row order: row i takes the smallest
+// colour not used by any row that shares a column with it.  colT is the
+// column -> rows pattern (transpose).
+inline int dist2_color(int64_t n, int64_t ncols, const std::vector<int64_t>& rp,
+                       const std::vector<int32_t>& col, std::vector<int32_t>& color)
+{
+  std::vector<int64_t> tp(ncols + 1, 0);
+  for (int64_t p = 0; p < rp[n]; p++) tp[col[p] + 1]++;
+  for (int64_t j = 0; j < ncols; j++) tp[j + 1] += tp[j];
+  std::vector<int32_t> trow(rp[n]);
+  {
+    std::vector<int64_t> fill(tp.begin(), tp.end() - 1);
+    for (int64_t i = 0; i < n; i++)
+      for (int64_t p = rp[i]; p < rp[i + 1]; p++) trow[fill[col[p]]++] = (int32_t)i;
+  }
+  color.assign(n, -1);
+  std::vector<int64_t> mark;  // mark[c] == i: colour c forbidden for row i
+  int ncolor = 0;
+  for (int64_t i = 0; i < n; i++) {
+    for (int64_t p = rp[i]; p < rp[i + 1]; p++) {
+      const int32_t c = col[p];
+      for (int64_t t = tp[c]; t < tp[c + 1]; t++) {
+        const int32_t r = trow[t];
+        const int32_t cr = color[r];
+        if (r != i && cr >= 0) {
+          if ((int)mark.size() <= cr) mark.resize(cr + 1, -1);
+          mark[cr] = i;
+        }
+      }
+    }
+    int c = 0;
+    while (c < (int)mark.size() && mark[c] == i) c++;
+    color[i] = c;
+    if (c + 1 > ncolor) ncolor = c + 1;
+  }
+  return ncolor;
+}
+
+}  // namespace pb

@@ -1,0 +1,286 @@
+// pb_spmmv.cuh -- SELL-C-sigma sparse matrix times row-major block vector.
+//
+//   Y = alpha*(A + diag(shifts)) X + beta*Y          (sparseMat_times_mvec*,
+//                                                     phist_kernels_decl.h:651-667)
+//   optional epilogues in the same pass:
+//     WdotW[j] = Y_j'Y_j,  VdotW[j] = X_j'Y_j          (fused_spmv_mvdot)
+//     U = gamma*Y + delta*U                           (fused_spmv_mvdot_mvadd)
+//   (phist_kernels_fused_decl.h:45-80)
+//
+// Thread mapping: a SELL row is handled by TPR consecutive threads, each
+// owning VPT of the block vector's columns; the row's entries are streamed
+// chunk-column by chunk-column (val/col reads are coalesced across the C rows
+// of a chunk), the X rows they address are gathered with 16-byte vector loads
+// (columns interleaved across the TPR threads so one warp-wide load covers a
+// contiguous segment of each X row).  Arithmetic follows the builtin loop of
+// spmvm_kernels.F90:494-523: tmp = shift*x_i, then the row's entries in stored
+// order, then y = alpha*tmp + beta*y.
+#pragma once
+#include "pb_core.hpp"
+#include "pb_reduce.cuh"
+
+namespace pb {
+
+template <class T>
+struct SellDev {
+  int64_t nrows;      // original rows
+  int64_t nchunks;
+  int C;
+  const int64_t* __restrict__ chunk_ptr;
+  const int32_t* __restrict__ chunk_len;
+  const int32_t* __restrict__ col;
+  const T* __restrict__ val;
+  const int32_t* __restrict__ perm;  // nullptr: identity
+};
+
+template <class T>
+struct SpmvArgs {
+  T alpha, beta;
+  int has_shift;                 // shifts sh[0..nvec) present
+  T sh[32];                      // per-column shifts of this column tile
+  const T* __restrict__ x;
+  int64_t ldx;
+  T* y;
+  int64_t ldy;
+  int nvec;                      // columns actually present (<= NV)
+  int col0;                      // first column of this launch (column tiles)
+  // epilogues
+  int want_wdw, want_vdw;
+  T* part;                       // per-block partials [grid][2*NV]
+  unsigned int* counter;
+  T* dots_out;                   // device [2*NV]: WdotW then VdotW
+  T gamma, delta;
+  T* u;
+  int64_t ldu;
+};
+
+template <class T, int W>
+struct VecLd;
+template <>
+struct VecLd<double, 2> {
+  static __device__ __forceinline__ void ld(const double* p, double* o)
+  {
+    double2 v = __ldg(reinterpret_cast<const double2*>(p));
+    o[0] = v.x; o[1] = v.y;
+  }
+  static __device__ __forceinline__ void ld_plain(const double* p, double* o)
+  {
+    double2 v = *reinterpret_cast<const double2*>(p);
+    o[0] = v.x; o[1] = v.y;
+  }
+  static __device__ __forceinline__ void st(double* p, const double* o)
+  {
+    *reinterpret_cast<double2*>(p) = make_double2(o[0], o[1]);
+  }
+};
+template <>
+struct VecLd<float, 4> {
+  static __device__ __forceinline__ void ld(const float* p, float* o)
+  {
+    float4 v = __ldg(reinterpret_cast<const float4*>(p));
+    o[0] = v.x; o[1] = v.y; o[2] = v.z; o[3] = v.w;
+  }
+  static __device__ __forceinline__ void ld_plain(const float* p, float* o)
+  {
+    float4 v = *reinterpret_cast<const float4*>(p);
+    o[0] = v.x; o[1] = v.y; o[2] = v.z; o[3] = v.w;
+  }
+  static __device__ __forceinline__ void st(float* p, const float* o)
+  {
+    *reinterpret_cast<float4*>(p) = make_float4(o[0], o[1], o[2], o[3]);
+  }
+};
+template <>
+struct VecLd<float, 2> {
+  static __device__ __forceinline__ void ld(const float* p, float* o)
+  {
+    float2 v = __ldg(reinterpret_cast<const float2*>(p));
+    o[0] = v.x; o[1] = v.y;
+  }
+  static __device__ __forceinline__ void ld_plain(const float* p, float* o)
+  {
+    float2 v = *reinterpret_cast<const float2*>(p);
+    o[0] = v.x; o[1] = v.y;
+  }
+  static __device__ __forceinline__ void st(float* p, const float* o)
+  {
+    *reinterpret_cast<float2*>(p) = make_float2(o[0], o[1]);
+  }
+};
+template <class T>
+struct VecLd1 {
+  static __device__ __forceinline__ void ld(const T* p, T* o) { o[0] = __ldg(p); }
+  static __device__ __forceinline__ void ld_plain(const T* p, T* o) { o[0] = *p; }
+  static __device__ __forceinline__ void st(T* p, const T* o) { *p = o[0]; }
+};
+template <class T, int W>
+struct Vec : VecLd<T, W> {};
+template <>
+struct Vec<double, 1> : VecLd1<double> {};
+template <>
+struct Vec<float, 1> : VecLd1<float> {};
+
+// column handled by (lane-in-row s, vector v, element w)
+template <int TPR, int VW>
+__device__ __forceinline__ int spmv_col(int s, int v, int w)
+{
+  return VW * (s + v * TPR) + w;
+}
+
+constexpr int SPMV_BS = 256;
+
+template <class T, int NV, int TPR, bool VEC>
+__global__ void __launch_bounds__(SPMV_BS)
+k_sell_spmmv(SellDev<T> A, SpmvArgs<T> p)
+{
+  constexpr int VPT = NV / TPR;                              // columns per thread
+  constexpr int VWMAX = 16 / sizeof(T);
+  constexpr int VW = VEC ? (VPT < VWMAX ? VPT : VWMAX) : 1;  // vector width
+  constexpr int NVV = VPT / VW;                               // vectors per thread
+  constexpr int RPB = SPMV_BS / TPR;                          // rows per block
+  typedef typename Acc<T>::type AT;
+
+  const int tid = threadIdx.x;
+  const int s = tid % TPR;
+  const int64_t r = (int64_t)blockIdx.x * RPB + tid / TPR;  // SELL row
+  const int C = A.C;
+  const int64_t i = (r < A.nrows) ? (A.perm ? (int64_t)A.perm[r] : r) : -1;
+  const int nv = p.nvec;
+  const T* __restrict__ x = p.x + p.col0;
+
+  AT acc[VPT];
+  T xi[VPT];
+#pragma unroll
+  for (int q = 0; q < VPT; q++) { acc[q] = AT(0); xi[q] = T(0); }
+
+  if (i >= 0 && (p.has_shift || p.want_vdw)) {
+#pragma unroll
+    for (int v = 0; v < NVV; v++) {
+      const int c = spmv_col<TPR, VW>(s, v, 0);
+      if (VEC || c < nv) Vec<T, VW>::ld(x + i * p.ldx + c, &xi[v * VW]);
+    }
+    if (p.has_shift) {
+#pragma unroll
+      for (int v = 0; v < NVV; v++)
+#pragma unroll
+        for (int w = 0; w < VW; w++) {
+          const int c = spmv_col<TPR, VW>(s, v, w);
+          if (VEC || c < nv) acc[v * VW + w] = AT(p.sh[c]) * AT(xi[v * VW + w]);
+        }
+    }
+  }
+
+  if (r < A.nchunks * (int64_t)C) {
+    const int64_t ch = r / C;
+    const int l = (int)(r - ch * C);
+    const int64_t base = A.chunk_ptr[ch] + l;
+    const int len = A.chunk_len[ch];
+#pragma unroll 4
+    for (int k = 0; k < len; k++) {
+      const T a = __ldcs(A.val + base + (int64_t)k * C);
+      const int64_t cj = __ldcs(A.col + base + (int64_t)k * C);
+      const T* xr = x + cj * p.ldx;
+#pragma unroll
+      for (int v = 0; v < NVV; v++) {
+        const int c = spmv_col<TPR, VW>(s, v, 0);
+        if (VEC || c < nv) {
+          T xv[VW];
+          Vec<T, VW>::ld(xr + c, xv);
+#pragma unroll
+          for (int w = 0; w < VW; w++) acc[v * VW + w] += AT(a) * AT(xv[w]);
+        }
+      }
+    }
+  }
+
+  T wdw[VPT], vdw[VPT];
+#pragma unroll
+  for (int q = 0; q < VPT; q++) { wdw[q] = T(0); vdw[q] = T(0); }
+
+  if (i >= 0) {
+    T* yr = p.y + p.col0 + i * p.ldy;
+#pragma unroll
+    for (int v = 0; v < NVV; v++) {
+      const int c = spmv_col<TPR, VW>(s, v, 0);
+      if (!(VEC || c < nv)) continue;
+      T yv[VW];
+      if (p.beta != T(0)) {
+        Vec<T, VW>::ld_plain(yr + c, yv);
+#pragma unroll
+        for (int w = 0; w < VW; w++) yv[w] = T(AT(p.alpha) * acc[v * VW + w] + AT(p.beta) * AT(yv[w]));
+      } else {
+#pragma unroll
+        for (int w = 0; w < VW; w++) yv[w] = T(AT(p.alpha) * acc[v * VW + w]);
+      }
+      Vec<T, VW>::st(yr + c, yv);
+#pragma unroll
+      for (int w = 0; w < VW; w++) {
+        wdw[v * VW + w] = yv[w] * yv[w];
+        vdw[v * VW + w] = xi[v * VW + w] * yv[w];
+      }
+      if (p.u) {
+        T* ur = p.u + p.col0 + i * p.ldu + c;
+        T uv[VW];
+        if (p.delta != T(0)) {
+          Vec<T, VW>::ld_plain(ur, uv);
+#pragma unroll
+          for (int w = 0; w < VW; w++) uv[w] = p.gamma * yv[w] + p.delta * uv[w];
+        } else {
+#pragma unroll
+          for (int w = 0; w < VW; w++) uv[w] = p.gamma * yv[w];
+        }
+        Vec<T, VW>::st(ur, uv);
+      }
+    }
+  }
+
+  if (!(p.want_wdw || p.want_vdw)) return;
+
+  // ---- block reduction of the column dots, fixed order ----
+  // lanes with equal s hold the same columns: butterfly over offsets >= TPR
+#pragma unroll
+  for (int off = 16; off >= TPR; off >>= 1) {
+#pragma unroll
+    for (int q = 0; q < VPT; q++) {
+      wdw[q] += __shfl_xor_sync(0xffffffffu, wdw[q], off);
+      vdw[q] += __shfl_xor_sync(0xffffffffu, vdw[q], off);
+    }
+  }
+  constexpr int NW = SPMV_BS / 32;
+  __shared__ T red[NW][2 * NV];
+  const int lane = tid & 31, warp = tid >> 5;
+  if (lane < TPR) {
+#pragma unroll
+    for (int v = 0; v < NVV; v++)
+#pragma unroll
+      for (int w = 0; w < VW; w++) {
+        const int c = spmv_col<TPR, VW>(lane, v, w);
+        red[warp][c] = wdw[v * VW + w];
+        red[warp][NV + c] = vdw[v * VW + w];
+      }
+  }
+  __syncthreads();
+  T* part = p.part + (int64_t)blockIdx.x * 2 * NV;
+  if (tid < 2 * NV) {
+    T sacc = T(0);
+#pragma unroll
+    for (int w = 0; w < NW; w++) sacc += red[w][tid];
+    part[tid] = sacc;
+  }
+  last_block_reduce<T>(p.part, 2 * NV, gridDim.x, p.counter, p.dots_out, 1, 2 * NV, 0, T(1), T(0));
+}
+
+// alpha == 0 / empty matrix: Y = beta*Y (crsmat_module.F90:1508-1511)
+template <class T>
+__global__ void k_scale_rows(T* y, int64_t ldy, int64_t n, int nvec, T beta)
+{
+  const int64_t tot = n * nvec;
+  for (int64_t t = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; t < tot;
+       t += (int64_t)gridDim.x * blockDim.x) {
+    const int64_t i = t / nvec;
+    const int j = (int)(t - i * nvec);
+    y[i * ldy + j] = (beta == T(0)) ? T(0) : beta * y[i * ldy + j];
+  }
+}
+
+}  // namespace pb

@@ -1,0 +1,133 @@
+"""CARP sweeps on the GPU (carp_setup / carp_sweep / carp_destroy).
+
+The GPU sweep runs colour class by colour class of a distance-2 colouring;
+it must equal the oracle's sequential Kaczmarz sweep over the same row order
+(kacz_sub_def.h update formulae) to rounding, the colouring must be a valid
+distance-2 colouring, repeated sweeps must be bitwise reproducible (the
+reference's CarpTest checks repeatability, CarpTest_def.hpp:579-611), and
+sweeps must drive the residual of (A - sigma I) x = b down.
+"""
+import ctypes as ct
+
+import numpy as np
+import pytest
+
+from conftest import relerr
+
+pytestmark = pytest.mark.gpu
+
+
+def _setup(A, shifts, dtype=np.float64):
+    from phist_b200 import kernels as K
+    from phist_b200.objects import fn
+    work = ct.c_void_p()
+    sh = np.ascontiguousarray(shifts, dtype)
+    K.chk(fn(dtype, "carp_setup"), A.h, len(sh), K.sptr(sh, dtype), ct.byref(work))
+    return work, sh
+
+
+def _order(work, n):
+    from phist_b200 import kernels as K
+    rows = np.zeros(n, np.int32)
+    nc = ct.c_int()
+    K.chk(K.phist_b200_Dcarp_color_order, work, K.ptr(rows), ct.byref(nc), None)
+    cp = np.zeros(nc.value + 1, np.int64)
+    K.chk(K.phist_b200_Dcarp_color_order, work, None, None, K.ptr(cp))
+    return rows, cp
+
+
+@pytest.mark.parametrize("prob,nvec", [("sprandn388", 1), ("sprandn388", 4), ("symmMat20", 3),
+                                       ("spshift388", 8), ("jadaTestMat512", 2)])
+def test_carp_sweep_vs_oracle(session, oracle, testmats, prob, nvec):
+    from phist_b200 import kernels as K
+    from phist_b200.objects import Mvec, SparseMat
+    rp, c, v, shape = testmats(prob)
+    A = SparseMat.from_crs(rp, c, v, ncols=shape[1])
+    n = shape[0]
+    rng = np.random.default_rng(nvec)
+    shifts = rng.uniform(-1, 1, nvec)
+    omega = rng.uniform(0.8, 1.6, nvec)
+    x0 = rng.uniform(-1, 1, (n, nvec))
+    b = rng.uniform(-1, 1, (n, nvec))
+    work, sh = _setup(A, shifts)
+    rows, cp = _order(work, n)
+    assert sorted(rows) == list(range(n))
+    colour = np.zeros(n, np.int32)
+    for k in range(len(cp) - 1):
+        colour[rows[cp[k]:cp[k + 1]]] = k
+    assert oracle.check_dist2(rp, c, shape[1], colour) == 0
+    X = Mvec(A.row_map, nvec).set(x0)
+    B = Mvec(A.row_map, nvec).set(b)
+    K.chk(K.phist_Dcarp_sweep, A.h, K.sptr(sh, np.float64), B.h, X.h, work, K.sptr(omega, np.float64))
+    ref = oracle.carp_sweep(rp, c, v, shifts, b, x0, omega, order=rows)
+    assert relerr(X.get(), ref) < 1e-13
+    # rhs NULL means b = 0
+    X.set(x0)
+    K.chk(K.phist_Dcarp_sweep, A.h, K.sptr(sh, np.float64), None, X.h, work, K.sptr(omega, np.float64))
+    ref0 = oracle.carp_sweep(rp, c, v, shifts, None, x0, omega, order=rows)
+    assert relerr(X.get(), ref0) < 1e-13
+    # repeatability
+    X.set(x0)
+    K.chk(K.phist_Dcarp_sweep, A.h, K.sptr(sh, np.float64), B.h, X.h, work, K.sptr(omega, np.float64))
+    again = X.get()
+    X.set(x0)
+    K.chk(K.phist_Dcarp_sweep, A.h, K.sptr(sh, np.float64), B.h, X.h, work, K.sptr(omega, np.float64))
+    assert np.array_equal(again, X.get())
+    K.chk(K.phist_Dcarp_destroy, A.h, work)
+    for o in (X, B, A):
+        o.delete()
+
+
+def test_carp_converges_honeycomb(session, oracle):
+    """many sweeps on the shifted honeycomb operator reduce the residual of
+    the normal equations; real shifts inside the spectrum"""
+    from phist_b200 import generators as G
+    from phist_b200 import kernels as K
+    from phist_b200.objects import Mvec, SparseMat
+    rp, c, v = G.honeycomb(24, 24, 4)
+    n = len(rp) - 1
+    A = SparseMat.from_crs(rp, c, v)
+    nvec = 4
+    shifts = np.array([-2.0, -0.5, 0.7, 2.2])
+    omega = np.ones(nvec)
+    b = G.random_block(n, nvec, 11)
+    work, sh = _setup(A, shifts)
+    X = Mvec(A.row_map, nvec)
+    B = Mvec(A.row_map, nvec).set(b)
+    for _ in range(200):
+        K.chk(K.phist_Dcarp_sweep, A.h, K.sptr(sh, np.float64), B.h, X.h, work, K.sptr(omega, np.float64))
+    x = X.get()
+    r = b - oracle.spmmv(rp, c, v, x, shifts=-shifts)
+    assert np.all(np.linalg.norm(r, axis=0) < 0.3 * np.linalg.norm(b, axis=0))
+    K.chk(K.phist_Dcarp_destroy, A.h, work)
+    for o in (X, B, A):
+        o.delete()
+
+
+def test_carp_rc_reduces_to_real(session, oracle, testmats):
+    """complex-shift variant with zero imaginary parts equals the real sweep"""
+    from phist_b200 import kernels as K
+    from phist_b200.objects import Mvec, SparseMat
+    rp, c, v, shape = testmats("sprandn388")
+    A = SparseMat.from_crs(rp, c, v)
+    n, nvec = 388, 2
+    sr = np.array([0.3, -0.4])
+    si = np.zeros(2)
+    om = np.array([1.0, 1.2])
+    rng = np.random.default_rng(3)
+    x0 = rng.uniform(-1, 1, (n, nvec))
+    b = rng.uniform(-1, 1, (n, nvec))
+    work = ct.c_void_p()
+    K.chk(K.phist_Dcarp_setup_rc, A.h, 2, K.sptr(sr, np.float64), K.sptr(si, np.float64), ct.byref(work))
+    rows, _ = _order(work, n)
+    Xr = Mvec(A.row_map, nvec).set(x0)
+    Xi = Mvec(A.row_map, nvec)
+    B = Mvec(A.row_map, nvec).set(b)
+    K.chk(K.phist_Dcarp_sweep_rc, A.h, K.sptr(sr, np.float64), K.sptr(si, np.float64), B.h, Xr.h, Xi.h,
+          work, K.sptr(om, np.float64))
+    ref = oracle.carp_sweep(rp, c, v, sr, b, x0, om, order=rows)
+    assert relerr(Xr.get(), ref) < 1e-13
+    assert np.abs(Xi.get()).max() == 0.0
+    K.chk(K.phist_Dcarp_destroy, A.h, work)
+    for o in (Xr, Xi, B, A):
+        o.delete()
