@@ -567,8 +567,17 @@ struct SpmvOut {
   bool wdw = false, vdw = false;
 };
 
+template <class T, int NV, int TPR, int KMAX>
+void launch_spmv_k(const SellDev<T>& S, SpmvArgs<T>& p, int grid, bool vec)
+{
+  if (vec)
+    k_sell_spmmv<T, NV, TPR, true, KMAX><<<grid, SPMV_BS, 0, stream()>>>(S, p);
+  else
+    k_sell_spmmv<T, NV, TPR, false, KMAX><<<grid, SPMV_BS, 0, stream()>>>(S, p);
+}
+
 template <class T, int NV, int TPR>
-void launch_spmv_nv(const SellDev<T>& S, SpmvArgs<T>& p, int64_t nrows_padded, bool vec)
+void launch_spmv_nv(const SellDev<T>& S, SpmvArgs<T>& p, int64_t nrows_padded, bool vec, int maxlen)
 {
   constexpr int RPB = SPMV_BS / TPR;
   const int grid = (int)ceil_div(nrows_padded > 0 ? nrows_padded : 1, RPB);
@@ -576,10 +585,13 @@ void launch_spmv_nv(const SellDev<T>& S, SpmvArgs<T>& p, int64_t nrows_padded, b
     p.part = (T*)rt().scratch(sizeof(T) * (size_t)grid * 2 * NV);
     p.counter = rt().counters();
   }
-  if (vec)
-    k_sell_spmmv<T, NV, TPR, true><<<grid, SPMV_BS, 0, stream()>>>(S, p);
+  // short rows (stencils, lattices): fully unrolled row loop
+  if (maxlen <= 8)
+    launch_spmv_k<T, NV, TPR, 8>(S, p, grid, vec);
+  else if (maxlen <= 16 && NV <= 8)
+    launch_spmv_k<T, NV, TPR, 16>(S, p, grid, vec);
   else
-    k_sell_spmmv<T, NV, TPR, false><<<grid, SPMV_BS, 0, stream()>>>(S, p);
+    launch_spmv_k<T, NV, TPR, 0>(S, p, grid, vec);
   PB_LAUNCH_CHECK();
 }
 
@@ -608,21 +620,21 @@ void spmv_tile(const SparseMat<T>* A, SpmvArgs<T>& p, int nv)
   }
   if (sizeof(T) == 8) {
     switch (NV) {
-      case 1: launch_spmv_nv<T, 1, 1>(S, p, npad, false); break;
-      case 2: launch_spmv_nv<T, 2, 1>(S, p, npad, vec); break;
-      case 4: launch_spmv_nv<T, 4, 1>(S, p, npad, vec); break;
-      case 8: launch_spmv_nv<T, 8, 2>(S, p, npad, vec); break;
-      case 16: launch_spmv_nv<T, 16, 4>(S, p, npad, vec); break;
-      default: launch_spmv_nv<T, 32, 8>(S, p, npad, vec); break;
+      case 1: launch_spmv_nv<T, 1, 1>(S, p, npad, false, A->max_row_len); break;
+      case 2: launch_spmv_nv<T, 2, 1>(S, p, npad, vec, A->max_row_len); break;
+      case 4: launch_spmv_nv<T, 4, 1>(S, p, npad, vec, A->max_row_len); break;
+      case 8: launch_spmv_nv<T, 8, 2>(S, p, npad, vec, A->max_row_len); break;
+      case 16: launch_spmv_nv<T, 16, 4>(S, p, npad, vec, A->max_row_len); break;
+      default: launch_spmv_nv<T, 32, 8>(S, p, npad, vec, A->max_row_len); break;
     }
   } else {
     switch (NV) {
-      case 1: launch_spmv_nv<T, 1, 1>(S, p, npad, false); break;
-      case 2: launch_spmv_nv<T, 2, 1>(S, p, npad, false); break;
-      case 4: launch_spmv_nv<T, 4, 1>(S, p, npad, vec); break;
-      case 8: launch_spmv_nv<T, 8, 2>(S, p, npad, vec); break;
-      case 16: launch_spmv_nv<T, 16, 4>(S, p, npad, vec); break;
-      default: launch_spmv_nv<T, 32, 8>(S, p, npad, vec); break;
+      case 1: launch_spmv_nv<T, 1, 1>(S, p, npad, false, A->max_row_len); break;
+      case 2: launch_spmv_nv<T, 2, 1>(S, p, npad, false, A->max_row_len); break;
+      case 4: launch_spmv_nv<T, 4, 1>(S, p, npad, vec, A->max_row_len); break;
+      case 8: launch_spmv_nv<T, 8, 2>(S, p, npad, vec, A->max_row_len); break;
+      case 16: launch_spmv_nv<T, 16, 4>(S, p, npad, vec, A->max_row_len); break;
+      default: launch_spmv_nv<T, 32, 8>(S, p, npad, vec, A->max_row_len); break;
     }
   }
 }
@@ -812,8 +824,23 @@ CarpWork<T>* carp_build(const SparseMat<T>* A, int nshifts, const T* sr, const T
   if (si) w->sigma_i.assign(si, si + nshifts);
   else w->sigma_i.assign(nshifts, T(0));
   const int64_t n = A->nrows;
+  // The projection of row i also writes x_i through the shift term
+  // (x_i += tmp*sigma) even where row i stores no diagonal entry, so the
+  // colouring works on the pattern of A with every diagonal present.
+  std::vector<int64_t> prp(n + 1, 0);
+  std::vector<int32_t> pcol;
+  pcol.reserve(A->nnz + n);
+  for (int64_t i = 0; i < n; i++) {
+    bool has_diag = false;
+    for (int64_t p = A->h_row_ptr[i]; p < A->h_row_ptr[i + 1]; p++) {
+      pcol.push_back(A->h_col[p]);
+      has_diag |= (A->h_col[p] == i);
+    }
+    if (!has_diag) pcol.push_back((int32_t)i);
+    prp[i + 1] = (int64_t)pcol.size();
+  }
   std::vector<int32_t> color;
-  w->ncolors = dist2_color(n, A->ncols, A->h_row_ptr, A->h_col, color);
+  w->ncolors = dist2_color(n, A->ncols, prp, pcol, color);
   w->h_color_ptr.assign(w->ncolors + 1, 0);
   for (int64_t i = 0; i < n; i++) w->h_color_ptr[color[i] + 1]++;
   for (int c = 0; c < w->ncolors; c++) w->h_color_ptr[c + 1] += w->h_color_ptr[c];

@@ -129,7 +129,9 @@ __device__ __forceinline__ int spmv_col(int s, int v, int w)
 
 constexpr int SPMV_BS = 256;
 
-template <class T, int NV, int TPR, bool VEC>
+// KMAX > 0: every chunk of the matrix is at most KMAX entries long (fully
+// unrolled row loop); KMAX == 0: any length (runtime loop)
+template <class T, int NV, int TPR, bool VEC, int KMAX>
 __global__ void __launch_bounds__(SPMV_BS)
 k_sell_spmmv(SellDev<T> A, SpmvArgs<T> p)
 {
@@ -170,7 +172,43 @@ k_sell_spmmv(SellDev<T> A, SpmvArgs<T> p)
     }
   }
 
-  if (r < A.nchunks * (int64_t)C) {
+  if (KMAX > 0 && r < A.nchunks * (int64_t)C) {
+    // chunk length <= KMAX: every entry's val/col load of the row is issued
+    // first, then every X-row gather, then the FMAs in entry order -- the
+    // loads of one row are all in flight together
+    const int64_t ch = r / C;
+    const int l = (int)(r - ch * C);
+    const int64_t base = A.chunk_ptr[ch] + l;
+    const int len = A.chunk_len[ch];
+    T av[KMAX > 0 ? KMAX : 1];
+    int cv[KMAX > 0 ? KMAX : 1];
+#pragma unroll
+    for (int k = 0; k < KMAX; k++) {
+      av[k] = T(0);
+      cv[k] = 0;
+      if (k < len) {
+        av[k] = __ldcs(A.val + base + (int64_t)k * C);
+        cv[k] = __ldcs(A.col + base + (int64_t)k * C);
+      }
+    }
+    T xv[KMAX > 0 ? KMAX : 1][VPT];
+#pragma unroll
+    for (int k = 0; k < KMAX; k++) {
+      const T* xr = x + (int64_t)cv[k] * p.ldx;
+#pragma unroll
+      for (int v = 0; v < NVV; v++) {
+        const int c = spmv_col<TPR, VW>(s, v, 0);
+#pragma unroll
+        for (int w = 0; w < VW; w++) xv[k][v * VW + w] = T(0);
+        if (k < len && (VEC || c < nv)) Vec<T, VW>::ld(xr + c, &xv[k][v * VW]);
+      }
+    }
+#pragma unroll
+    for (int k = 0; k < KMAX; k++)
+      if (k < len)
+#pragma unroll
+        for (int q = 0; q < VPT; q++) acc[q] += AT(av[k]) * AT(xv[k][q]);
+  } else if (r < A.nchunks * (int64_t)C) {
     const int64_t ch = r / C;
     const int l = (int)(r - ch * C);
     const int64_t base = A.chunk_ptr[ch] + l;

@@ -26,6 +26,18 @@ def _setup(A, shifts, dtype=np.float64):
     return work, sh
 
 
+def _with_diagonal(rp, c):
+    cols = []
+    prp = [0]
+    for i in range(len(rp) - 1):
+        row = list(c[rp[i]:rp[i + 1]])
+        if i not in row:
+            row.append(i)
+        cols.extend(row)
+        prp.append(len(cols))
+    return np.array(prp, np.int64), np.array(cols, np.int32)
+
+
 def _order(work, n):
     from phist_b200 import kernels as K
     rows = np.zeros(n, np.int32)
@@ -37,7 +49,8 @@ def _order(work, n):
 
 
 @pytest.mark.parametrize("prob,nvec", [("sprandn388", 1), ("sprandn388", 4), ("symmMat20", 3),
-                                       ("spshift388", 8), ("jadaTestMat512", 2)])
+                                       ("spshift388", 8), ("jadaTestMat512", 2),
+                                       ("sprandn_nodiag388", 4), ("spshift25", 1)])
 def test_carp_sweep_vs_oracle(session, oracle, testmats, prob, nvec):
     from phist_b200 import kernels as K
     from phist_b200.objects import Mvec, SparseMat
@@ -55,7 +68,9 @@ def test_carp_sweep_vs_oracle(session, oracle, testmats, prob, nvec):
     colour = np.zeros(n, np.int32)
     for k in range(len(cp) - 1):
         colour[rows[cp[k]:cp[k + 1]]] = k
-    assert oracle.check_dist2(rp, c, shape[1], colour) == 0
+    # the shift term writes x_i, so every row's own index belongs to its pattern
+    prp, pcol = _with_diagonal(rp, c)
+    assert oracle.check_dist2(prp, pcol, shape[1], colour) == 0
     X = Mvec(A.row_map, nvec).set(x0)
     B = Mvec(A.row_map, nvec).set(b)
     K.chk(K.phist_Dcarp_sweep, A.h, K.sptr(sh, np.float64), B.h, X.h, work, K.sptr(omega, np.float64))
