@@ -352,6 +352,11 @@ int phist_b200_problem_rowfunc(phist_gidx row, phist_lidx* len, phist_gidx* cols
 /* SELL chunk height C (1..32, power of two) and the sigma window used when a
  * matrix is built with PHIST_SPARSEMAT_PERM_LOCAL (<=1: no sorting) */
 void phist_b200_set_sell_params(int C, int64_t sigma, int* iflag);
+/* SpMMV launch shape (autotuning control): threads per matrix row for block
+ * width nvec (1,2,4,8,16,32; allowed pairs 1:1, 2:1, 4:1|2, 8:2|4, 16:4|8,
+ * 32:8|16) and, when unroll >= 0, whether the fully unrolled kernel for
+ * matrices whose rows have at most 8 entries may be used */
+void phist_b200_set_spmv_config(int nvec, int tpr, int unroll, int* iflag);
 /* wait for all work this library enqueued */
 void phist_b200_synchronize(int* iflag);
 /* number of kernel launches this library has issued since init */

@@ -96,6 +96,35 @@ def suite_spmmv(T, reps, peak, L=128):
     return out
 
 
+def suite_spmmv_tune(T, reps, peak, L=128):
+    """every SpMMV launch shape (threads per row, unrolled or not) per width"""
+    from . import kernels as K
+    from .generators import random_block
+    from .objects import Mvec, SparseMat
+    K.chk(K.phist_b200_set_sell_params, 32, 256)
+    A = SparseMat.from_problem("ANDERSON3D-%d-S1" % L, flags=K.PHIST_SPARSEMAT_PERM_LOCAL)
+    n, nnz = A.nrows, A.nnz
+    opts = {1: (1,), 2: (1,), 4: (1, 2), 8: (2, 4), 16: (4, 8), 32: (8, 16)}
+    out = []
+    for nv, tprs in opts.items():
+        X = Mvec(A.domain_map, nv).set(random_block(n, nv, 3))
+        Y = Mvec(A.row_map, nv)
+        b = nnz * 12 + 16 * n * nv + (-(-n // 32)) * 12
+        for tpr in tprs:
+            for unroll in (1, 0):
+                K.chk(K.phist_b200_set_spmv_config, nv, tpr, unroll)
+                t = T.time(lambda: K.chk(K.phist_DsparseMat_times_mvec, 1.0, A.h, X.h, 0.0, Y.h), reps)
+                out.append(report("spmmv_tpr%d_unroll%d" % (tpr, unroll), {"n": n, "nnz": nnz, "nvec": nv},
+                                  b, 2 * nnz * nv, t, peak))
+        X.delete()
+        Y.delete()
+    # back to the defaults
+    for nv, tpr in ((4, 1), (8, 2), (16, 4), (32, 8)):
+        K.chk(K.phist_b200_set_spmv_config, nv, tpr, 1)
+    A.delete()
+    return out
+
+
 def suite_block(T, reps, peak, n=1 << 21):
     from . import kernels as K
     from .generators import random_block

@@ -567,31 +567,31 @@ struct SpmvOut {
   bool wdw = false, vdw = false;
 };
 
-template <class T, int NV, int TPR, int KMAX>
-void launch_spmv_k(const SellDev<T>& S, SpmvArgs<T>& p, int grid, bool vec)
-{
-  if (vec)
-    k_sell_spmmv<T, NV, TPR, true, KMAX><<<grid, SPMV_BS, 0, stream()>>>(S, p);
-  else
-    k_sell_spmmv<T, NV, TPR, false, KMAX><<<grid, SPMV_BS, 0, stream()>>>(S, p);
-}
-
+// one instantiation family per (block width NV, threads per row TPR): the
+// fully unrolled short-row kernel when the matrix has C=32 chunks of at most
+// 8 entries, the general kernel otherwise
 template <class T, int NV, int TPR>
-void launch_spmv_nv(const SellDev<T>& S, SpmvArgs<T>& p, int64_t nrows_padded, bool vec, int maxlen)
+void launch_spmv_nv(const SparseMat<T>* A, const SellDev<T>& S, SpmvArgs<T>& p, bool vec)
 {
   constexpr int RPB = SPMV_BS / TPR;
-  const int grid = (int)ceil_div(nrows_padded > 0 ? nrows_padded : 1, RPB);
+  const int64_t npad = A->nchunks * (int64_t)A->C;
+  const int grid = (int)ceil_div(npad > 0 ? npad : 1, RPB);
   if (p.want_wdw || p.want_vdw) {
     p.part = (T*)rt().scratch(sizeof(T) * (size_t)grid * 2 * NV);
     p.counter = rt().counters();
   }
-  // short rows (stencils, lattices): fully unrolled row loop
-  if (maxlen <= 8)
-    launch_spmv_k<T, NV, TPR, 8>(S, p, grid, vec);
-  else if (maxlen <= 16 && NV <= 8)
-    launch_spmv_k<T, NV, TPR, 16>(S, p, grid, vec);
-  else
-    launch_spmv_k<T, NV, TPR, 0>(S, p, grid, vec);
+  const bool fast = rt().spmv_unroll && A->C == 32 && A->max_row_len <= 8;
+  if (fast) {
+    if (vec)
+      k_sell_spmmv<T, NV, TPR, true, 8, 32><<<grid, SPMV_BS, 0, stream()>>>(S, p);
+    else
+      k_sell_spmmv<T, NV, TPR, false, 8, 32><<<grid, SPMV_BS, 0, stream()>>>(S, p);
+  } else {
+    if (vec)
+      k_sell_spmmv<T, NV, TPR, true, 0, 0><<<grid, SPMV_BS, 0, stream()>>>(S, p);
+    else
+      k_sell_spmmv<T, NV, TPR, false, 0, 0><<<grid, SPMV_BS, 0, stream()>>>(S, p);
+  }
   PB_LAUNCH_CHECK();
 }
 
@@ -606,9 +606,9 @@ template <class T>
 void spmv_tile(const SparseMat<T>* A, SpmvArgs<T>& p, int nv)
 {
   const SellDev<T> S = sell_dev(A);
-  const int64_t npad = A->nchunks * (int64_t)A->C;
   p.nvec = nv;
-  int NV = nv <= 1 ? 1 : nv <= 2 ? 2 : nv <= 4 ? 4 : nv <= 8 ? 8 : nv <= 16 ? 16 : 32;
+  const int NV = nv <= 1 ? 1 : nv <= 2 ? 2 : nv <= 4 ? 4 : nv <= 8 ? 8 : nv <= 16 ? 16 : 32;
+  const int lg = NV == 1 ? 0 : NV == 2 ? 1 : NV == 4 ? 2 : NV == 8 ? 3 : NV == 16 ? 4 : 5;
   // vector path: the tile width is exactly NV and every row segment that a
   // thread touches starts on a 16-byte boundary
   const int vw = 16 / (int)sizeof(T);
@@ -618,24 +618,26 @@ void spmv_tile(const SparseMat<T>* A, SpmvArgs<T>& p, int nv)
           (p.ldy % vw == 0) && (!p.u || (aligned16<T>(p.u + p.col0) && p.ldu % vw == 0));
     if (sizeof(T) == 4 && NV == 2) vec = false;
   }
-  if (sizeof(T) == 8) {
-    switch (NV) {
-      case 1: launch_spmv_nv<T, 1, 1>(S, p, npad, false, A->max_row_len); break;
-      case 2: launch_spmv_nv<T, 2, 1>(S, p, npad, vec, A->max_row_len); break;
-      case 4: launch_spmv_nv<T, 4, 1>(S, p, npad, vec, A->max_row_len); break;
-      case 8: launch_spmv_nv<T, 8, 2>(S, p, npad, vec, A->max_row_len); break;
-      case 16: launch_spmv_nv<T, 16, 4>(S, p, npad, vec, A->max_row_len); break;
-      default: launch_spmv_nv<T, 32, 8>(S, p, npad, vec, A->max_row_len); break;
-    }
-  } else {
-    switch (NV) {
-      case 1: launch_spmv_nv<T, 1, 1>(S, p, npad, false, A->max_row_len); break;
-      case 2: launch_spmv_nv<T, 2, 1>(S, p, npad, false, A->max_row_len); break;
-      case 4: launch_spmv_nv<T, 4, 1>(S, p, npad, vec, A->max_row_len); break;
-      case 8: launch_spmv_nv<T, 8, 2>(S, p, npad, vec, A->max_row_len); break;
-      case 16: launch_spmv_nv<T, 16, 4>(S, p, npad, vec, A->max_row_len); break;
-      default: launch_spmv_nv<T, 32, 8>(S, p, npad, vec, A->max_row_len); break;
-    }
+  const int tpr = rt().spmv_tpr[lg];
+  switch (NV) {
+    case 1: launch_spmv_nv<T, 1, 1>(A, S, p, false); break;
+    case 2: launch_spmv_nv<T, 2, 1>(A, S, p, vec); break;
+    case 4:
+      if (tpr == 2) launch_spmv_nv<T, 4, 2>(A, S, p, vec);
+      else launch_spmv_nv<T, 4, 1>(A, S, p, vec);
+      break;
+    case 8:
+      if (tpr == 4) launch_spmv_nv<T, 8, 4>(A, S, p, vec);
+      else launch_spmv_nv<T, 8, 2>(A, S, p, vec);
+      break;
+    case 16:
+      if (tpr == 8) launch_spmv_nv<T, 16, 8>(A, S, p, vec);
+      else launch_spmv_nv<T, 16, 4>(A, S, p, vec);
+      break;
+    default:
+      if (tpr == 16) launch_spmv_nv<T, 32, 16>(A, S, p, vec);
+      else launch_spmv_nv<T, 32, 8>(A, S, p, vec);
+      break;
   }
 }
 
@@ -778,7 +780,8 @@ void launch_rowgemm(RowGemmArgs<T>& a)
   size_t smem = sizeof(T) * ((size_t)a.R * ap + (size_t)a.R * kp + (size_t)ap * kp +
                              (a.mode == RM_VCWD ? (size_t)kp * kp : 0) +
                              (a.gram == GM_VW ? (size_t)a.R * mvp : 0));
-  PB_REQUIRE(smem <= 227 * 1024, PB_NOT_IMPLEMENTED, "block product too wide for one tile (%zu bytes of shared memory)", smem);
+  // (plus the reduction's static shared buffer, 8 KiB)
+  PB_REQUIRE(smem + 9 * 1024 <= 227 * 1024, PB_NOT_IMPLEMENTED, "block product too wide for one tile (%zu bytes of shared memory)", smem);
   const int gm = (a.gram == GM_WW) ? a.k : a.mv;
   PB_REQUIRE(a.gram == GM_NONE || gm * a.k <= 16 * BLK_BS, PB_NOT_IMPLEMENTED, "fused Gram matrix larger than 64x64");
   const int64_t ntiles = ceil_div(a.n > 0 ? a.n : 1, a.R);

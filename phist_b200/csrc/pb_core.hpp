@@ -138,6 +138,11 @@ class Runtime {
   int64_t sell_sigma_default = 256;  // when PERM_LOCAL is requested
   int verbose = 0;
 
+  // SpMMV launch shape: threads per matrix row for block widths 1,2,4,8,16,32
+  // and whether the fully unrolled short-row kernel may be used
+  int spmv_tpr[6] = {1, 1, 1, 2, 4, 8};
+  bool spmv_unroll = true;
+
   // statistics: kernel launches issued by this library
   uint64_t launches = 0;
 

@@ -3,9 +3,12 @@
 // Level 1: every block reduces its threads' partial sums in a fixed order
 // and writes one partial vector to scratch[blockIdx.x][0..nout).
 // Level 2: the last block to finish (arrival counter) sums the partial
-// vectors in block order and writes the result.  The summation order never
-// depends on scheduling, so results are bitwise reproducible run to run for
-// a given launch shape.
+// vectors.  All of its threads take part: with G = blockDim/nout groups,
+// thread (g, o) sums the partials of blocks g, g+G, g+2G, ... in increasing
+// block order, then thread o adds the G group sums in increasing g.  The
+// summation order depends only on (nblocks, blockDim, nout), never on
+// scheduling, so results are bitwise reproducible run to run for a given
+// launch shape.
 #pragma once
 #include <cuda_runtime.h>
 
@@ -21,7 +24,8 @@ struct Acc<float> { typedef float type; };
 // Called by ALL threads of the block after the block partial has been written
 // to part[blockIdx.x*nout + o].  Returns true in the one block that performed
 // the final reduction (its threads wrote out[o] = alpha*sum + beta*out[o],
-// with out[o] not read when beta == 0).
+// with out[o] not read when beta == 0).  Output o goes to
+// out[(o % out_rows)*out_stride_rows + (o / out_rows)*ld_out].
 template <class T>
 __device__ __forceinline__ bool last_block_reduce(const T* part, int nout, int nblocks,
                                                   unsigned int* counter, T* out,
@@ -29,6 +33,7 @@ __device__ __forceinline__ bool last_block_reduce(const T* part, int nout, int n
                                                   int64_t ld_out, T alpha, T beta)
 {
   __shared__ bool am_last;
+  __shared__ T red[256];  // all callers launch at most 256 threads per block
   __threadfence();
   __syncthreads();
   if (threadIdx.x == 0) {
@@ -38,13 +43,44 @@ __device__ __forceinline__ bool last_block_reduce(const T* part, int nout, int n
   __syncthreads();
   if (!am_last) return false;
   __threadfence();
-  // out index o -> (row = o % out_rows, col = o / out_rows) for matrix outputs
-  for (int o = threadIdx.x; o < nout; o += blockDim.x) {
+  const int nt = blockDim.x;
+  const int G = (nout < nt) ? (nt / nout) : 1;  // groups of blocks
+  for (int o0 = 0; o0 < nout; o0 += nt) {
+    // thread t: output o = o0 + t % nout', group g = t / nout'
+    const int span = (nout - o0 < nt) ? (nout - o0) : nt;
+    const int g = threadIdx.x / span, oo = threadIdx.x - g * span;
     T s = T(0);
-    for (int b = 0; b < nblocks; b++) s += __ldcg(part + (int64_t)b * nout + o);
-    int r = o % out_rows, c = o / out_rows;
-    T* dst = out + r * out_stride_rows + (int64_t)c * ld_out;
-    *dst = (beta == T(0)) ? alpha * s : alpha * s + beta * (*dst);
+    if (g < G) {
+      const T* p = part + o0 + oo;
+      int b = g;
+      // 4 independent loads in flight, added in block order
+      for (; b + 3 * G < nblocks; b += 4 * G) {
+        const T v0 = __ldcg(p + (int64_t)b * nout);
+        const T v1 = __ldcg(p + (int64_t)(b + G) * nout);
+        const T v2 = __ldcg(p + (int64_t)(b + 2 * G) * nout);
+        const T v3 = __ldcg(p + (int64_t)(b + 3 * G) * nout);
+        s += v0;
+        s += v1;
+        s += v2;
+        s += v3;
+      }
+      for (; b < nblocks; b += G) s += __ldcg(p + (int64_t)b * nout);
+    }
+    if (G > 1) {
+      __syncthreads();
+      if (g < G) red[g * span + oo] = s;
+      __syncthreads();
+      if (threadIdx.x < span) {
+        s = T(0);
+        for (int gg = 0; gg < G; gg++) s += red[gg * span + threadIdx.x];
+      }
+    }
+    if (threadIdx.x < span) {
+      const int o = o0 + threadIdx.x;
+      const int r = o % out_rows, c = o / out_rows;
+      T* dst = out + r * out_stride_rows + (int64_t)c * ld_out;
+      *dst = (beta == T(0)) ? alpha * s : alpha * s + beta * (*dst);
+    }
   }
   if (threadIdx.x == 0) *counter = 0u;  // ready for the next launch
   return true;

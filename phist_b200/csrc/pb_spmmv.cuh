@@ -130,8 +130,10 @@ __device__ __forceinline__ int spmv_col(int s, int v, int w)
 constexpr int SPMV_BS = 256;
 
 // KMAX > 0: every chunk of the matrix is at most KMAX entries long (fully
-// unrolled row loop); KMAX == 0: any length (runtime loop)
-template <class T, int NV, int TPR, bool VEC, int KMAX>
+// unrolled row loop); KMAX == 0: any length (runtime loop).
+// CC > 0: the chunk height is the compile-time constant CC (entry offsets
+// become immediates); CC == 0: read from A.C.
+template <class T, int NV, int TPR, bool VEC, int KMAX, int CC>
 __global__ void __launch_bounds__(SPMV_BS)
 k_sell_spmmv(SellDev<T> A, SpmvArgs<T> p)
 {
@@ -145,7 +147,7 @@ k_sell_spmmv(SellDev<T> A, SpmvArgs<T> p)
   const int tid = threadIdx.x;
   const int s = tid % TPR;
   const int64_t r = (int64_t)blockIdx.x * RPB + tid / TPR;  // SELL row
-  const int C = A.C;
+  const int C = CC > 0 ? CC : A.C;
   const int64_t i = (r < A.nrows) ? (A.perm ? (int64_t)A.perm[r] : r) : -1;
   const int nv = p.nvec;
   const T* __restrict__ x = p.x + p.col0;
