@@ -348,6 +348,22 @@ void phist_b200_Screate_problem(phist_SsparseMat_ptr* A, phist_const_comm_ptr co
 void* phist_b200_problem_create(const char* problem, int single, int64_t* nrows, int32_t* maxnne);
 int phist_b200_problem_rowfunc(phist_gidx row, phist_lidx* len, phist_gidx* cols, void* vals, void* arg);
 
+/* No counterpart in PHIST.  C = alpha*V'W + beta*C (as phist_DmvecT_times_mvec)
+ * on raw DEVICE pointers, for callers that cannot allocate device memory
+ * (a host that fixes the device-memory budget at start-up and owns every later
+ * allocation, or that forbids cudaMalloc after initialisation).  It allocates
+ * nothing: its scratch is a fixed 4 MiB file-scope device array.
+ * V: n x m row-major (ldv >= m), W: n x k row-major (ldw >= k), C: m x k
+ * column-major (ldc >= m); 1 <= m, k <= 64, larger widths give *iflag = -55.
+ * stream: a cudaStream_t (NULL = legacy default stream).  The call is
+ * asynchronous on that stream.  The first call on a device does a one-time
+ * cudaGetSymbolAddress set-up; make it before any stream capture.  All calls
+ * share the scratch array: calls that overlap on the GPU race. */
+void phist_b200_DmvecT_times_mvec_noalloc(int64_t n, int m, int k, double alpha,
+                                          const double* V, int64_t ldv,
+                                          const double* W, int64_t ldw, double beta,
+                                          double* C, int64_t ldc, void* stream, int* iflag);
+
 /* runtime controls and statistics (library extensions) */
 /* SELL chunk height C (1..32, power of two) and the sigma window used when a
  * matrix is built with PHIST_SPARSEMAT_PERM_LOCAL (<=1: no sorting) */
