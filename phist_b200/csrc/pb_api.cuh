@@ -575,23 +575,26 @@ void launch_spmv_nv(const SparseMat<T>* A, const SellDev<T>& S, SpmvArgs<T>& p, 
 {
   constexpr int RPB = SPMV_BS / TPR;
   const int64_t npad = A->nchunks * (int64_t)A->C;
-  const int grid = (int)ceil_div(npad > 0 ? npad : 1, RPB);
+  int grid = (int)ceil_div(npad > 0 ? npad : 1, RPB);
   if (p.want_wdw || p.want_vdw) {
+    // fused dots: a bounded grid walks the row tiles, so few partial vectors
+    grid = std::min(grid, rt().num_sms() * 8);
     p.part = (T*)rt().scratch(sizeof(T) * (size_t)grid * 2 * NV);
     p.counter = rt().counters();
   }
   const bool fast = rt().spmv_unroll && A->C == 32 && A->max_row_len <= 8;
+  const bool dots = p.want_wdw || p.want_vdw;
+#define PB_SPMV(VECv, KMAXv, CCv)                                                         \
+  if (dots)                                                                             \
+    k_sell_spmmv<T, NV, TPR, VECv, KMAXv, CCv, true><<<grid, SPMV_BS, 0, stream()>>>(S, p); \
+  else                                                                                  \
+    k_sell_spmmv<T, NV, TPR, VECv, KMAXv, CCv, false><<<grid, SPMV_BS, 0, stream()>>>(S, p);
   if (fast) {
-    if (vec)
-      k_sell_spmmv<T, NV, TPR, true, 8, 32><<<grid, SPMV_BS, 0, stream()>>>(S, p);
-    else
-      k_sell_spmmv<T, NV, TPR, false, 8, 32><<<grid, SPMV_BS, 0, stream()>>>(S, p);
+    if (vec) { PB_SPMV(true, 8, 32) } else { PB_SPMV(false, 8, 32) }
   } else {
-    if (vec)
-      k_sell_spmmv<T, NV, TPR, true, 0, 0><<<grid, SPMV_BS, 0, stream()>>>(S, p);
-    else
-      k_sell_spmmv<T, NV, TPR, false, 0, 0><<<grid, SPMV_BS, 0, stream()>>>(S, p);
+    if (vec) { PB_SPMV(true, 0, 0) } else { PB_SPMV(false, 0, 0) }
   }
+#undef PB_SPMV
   PB_LAUNCH_CHECK();
 }
 
@@ -738,6 +741,23 @@ void launch_mvTmv(int64_t n, int m, int k, T alpha, const T* V, int64_t ldv, con
   MvTmvArgs<T> a;
   a.n = n; a.m = m; a.k = k; a.V = V; a.ldv = ldv; a.W = W; a.ldw = ldw;
   a.alpha = alpha; a.beta = beta; a.Cd = Cd; a.ldc = ldc;
+  if (m <= 8 && k <= 8) {
+    // register kernel: padded widths M (4|8) and K (1|4|8)
+    const int M = m <= 4 ? 4 : 8, K = k == 1 ? 1 : k <= 4 ? 4 : 8;
+    const int grid = std::max(1, std::min(grid_for(n), rt().num_sms() * 4));
+    a.part = (T*)rt().scratch(sizeof(T) * (size_t)grid * M * K);
+    a.counter = rt().counters();
+    a.R = 0;
+#define PB_MVR(Mv, Kv) k_mvTmv_reg<T, Mv, Kv><<<grid, 256, 0, stream()>>>(a)
+    if (M == 4) {
+      if (K == 1) PB_MVR(4, 1); else if (K == 4) PB_MVR(4, 4); else PB_MVR(4, 8);
+    } else {
+      if (K == 1) PB_MVR(8, 1); else if (K == 4) PB_MVR(8, 4); else PB_MVR(8, 8);
+    }
+#undef PB_MVR
+    PB_LAUNCH_CHECK();
+    return;
+  }
   const bool big = (int64_t)m * k >= 256;
   const int TM = big ? 8 : 4, TK = big ? 8 : 4;
   const int mp = ceil_div(m, TM) * TM, kp = ceil_div(k, TK) * TK;
@@ -768,6 +788,29 @@ void launch_mvTmv(int64_t n, int m, int k, T alpha, const T* V, int64_t ldv, con
 template <class T>
 void launch_rowgemm(RowGemmArgs<T>& a)
 {
+  if (a.m <= 8 && a.k <= 8 && (a.gram != GM_VW || a.mv <= 8)) {
+    // register kernel: padded widths M (4|8), K (1|4|8), MV (1, or 8 for V'W)
+    const int M = a.m <= 4 ? 4 : 8, K = a.k == 1 ? 1 : a.k <= 4 ? 4 : 8;
+    const int grid = std::max(1, std::min(grid_for(a.n), rt().num_sms() * 4));
+    if (a.gram != GM_NONE) {
+      a.part = (T*)rt().scratch(sizeof(T) * (size_t)grid * 64);
+      a.counter = rt().counters();
+    }
+#define PB_RGR(Mv, Kv, MVv) k_rowgemm_reg<T, Mv, Kv, MVv><<<grid, 256, 0, stream()>>>(a)
+#define PB_RGR_K(Mv, MVv)                                   \
+  if (K == 1) PB_RGR(Mv, 1, MVv);                           \
+  else if (K == 4) PB_RGR(Mv, 4, MVv);                      \
+  else PB_RGR(Mv, 8, MVv);
+    if (a.gram == GM_VW) {
+      if (M == 4) { PB_RGR_K(4, 8) } else { PB_RGR_K(8, 8) }
+    } else {
+      if (M == 4) { PB_RGR_K(4, 1) } else { PB_RGR_K(8, 1) }
+    }
+#undef PB_RGR_K
+#undef PB_RGR
+    PB_LAUNCH_CHECK();
+    return;
+  }
   // micro-tile: TK columns per thread, TR rows
   const int TK = a.k >= 32 ? 8 : a.k >= 8 ? 4 : a.k >= 2 ? 2 : 1;
   const int kp = ceil_div(a.k, TK) * TK;

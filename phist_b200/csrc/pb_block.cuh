@@ -32,6 +32,28 @@ __device__ __forceinline__ void stage_rows(T* s, int pitch, const T* __restrict_
                                            int64_t r0, int64_t n, int R, int ncols)
 {
   const int tot = R * pitch;
+  // rows stored back to back with the tile's own pitch and 16-byte aligned:
+  // one flat vectorised copy (the common case of a full, unpadded mvec)
+  constexpr int VW = 16 / sizeof(T);
+  if (ldg == pitch && pitch == ncols && ((uintptr_t)(g + r0 * ldg) & 15u) == 0 &&
+      ((uintptr_t)s & 15u) == 0 && (tot % VW) == 0) {
+    const int64_t avail = (n - r0) * (int64_t)pitch;  // elements inside the matrix
+    const T* src = g + r0 * ldg;
+    const int nv = tot / VW;
+    for (int t = threadIdx.x; t < nv; t += blockDim.x) {
+      const int64_t e = (int64_t)t * VW;
+      if (e + VW <= avail) {
+        if (sizeof(T) == 8) {
+          reinterpret_cast<double2*>(s)[t] = __ldcs(reinterpret_cast<const double2*>(src) + t);
+        } else {
+          reinterpret_cast<float4*>(s)[t] = __ldcs(reinterpret_cast<const float4*>(src) + t);
+        }
+      } else {
+        for (int w = 0; w < VW; w++) s[e + w] = (e + w < avail) ? src[e + w] : T(0);
+      }
+    }
+    return;
+  }
   for (int t = threadIdx.x; t < tot; t += blockDim.x) {
     const int rr = t / pitch, c = t - rr * pitch;
     const int64_t row = r0 + rr;
@@ -276,6 +298,138 @@ __global__ void __launch_bounds__(BLK_BS) k_rowgemm(RowGemmArgs<T> a)
   const T al = (a.gram == GM_WW) ? T(1) : a.galpha;
   const T be = (a.gram == GM_WW) ? T(0) : a.gbeta;
   last_block_reduce<T>(a.part, gout, gridDim.x, a.counter, a.Gd, 1, gm, a.ldg, al, be);
+}
+
+// ---------------------------------------------------- small widths (<= 8)
+// One thread per row, everything in registers: the row of V (M values) and
+// of W (K values) are loaded once, the M x K Gram contribution or the K new
+// values of W are formed in registers.  Used when m, k (and mv) are <= 8,
+// where the tiled kernels above would spend their time staging.
+
+template <class T>
+__device__ __forceinline__ void load_row(const T* __restrict__ p, int ncols, int NMAX, T* out)
+{
+  // NMAX compile-time at the call sites; columns >= ncols read as zero
+#pragma unroll
+  for (int c = 0; c < 8; c++)
+    if (c < NMAX) out[c] = (c < ncols) ? __ldg(p + c) : T(0);
+}
+
+// sum the NOUT per-thread values of every thread of the block in a fixed
+// order (warp butterfly, then warps in order) and write the block partial
+template <class T, int NOUT>
+__device__ __forceinline__ void block_partial(T* vals, T* part, int nout)
+{
+  __shared__ T red[8][NOUT];
+#pragma unroll
+  for (int off = 16; off >= 1; off >>= 1)
+#pragma unroll
+    for (int q = 0; q < NOUT; q++) vals[q] += __shfl_xor_sync(0xffffffffu, vals[q], off);
+  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+  if (lane == 0)
+#pragma unroll
+    for (int q = 0; q < NOUT; q++) red[warp][q] = vals[q];
+  __syncthreads();
+  for (int q = threadIdx.x; q < nout; q += blockDim.x) {
+    T s = T(0);
+    for (int w = 0; w < (int)(blockDim.x >> 5); w++) s += red[w][q];
+    part[(int64_t)blockIdx.x * nout + q] = s;
+  }
+}
+
+// C(m x k) = alpha V'W + beta C, m <= M, k <= K
+template <class T, int M, int K>
+__global__ void __launch_bounds__(256) k_mvTmv_reg(MvTmvArgs<T> a)
+{
+  T acc[M * K];
+#pragma unroll
+  for (int q = 0; q < M * K; q++) acc[q] = T(0);
+  for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < a.n;
+       i += (int64_t)gridDim.x * blockDim.x) {
+    T v[8], w[8];
+    load_row(a.V + i * a.ldv, a.m, M, v);
+    load_row(a.W + i * a.ldw, a.k, K, w);
+#pragma unroll
+    for (int q = 0; q < K; q++)
+#pragma unroll
+      for (int p = 0; p < M; p++) acc[p + q * M] += v[p] * w[q];
+  }
+  // compact to the m x k layout expected by the final reduction
+  T vals[M * K];
+#pragma unroll
+  for (int q = 0; q < K; q++)
+#pragma unroll
+    for (int p = 0; p < M; p++) vals[p + q * M] = acc[p + q * M];
+  block_partial<T, M * K>(vals, a.part, M * K);
+  // outputs are laid out with row stride M in the partials: map to (m, k)
+  last_block_reduce<T>(a.part, M * K, gridDim.x, a.counter, a.Cd, 1, M, a.ldc, a.alpha, a.beta, a.m, a.k);
+}
+
+// row-local products for m, k, mv <= 8 (modes and Gram as k_rowgemm)
+template <class T, int M, int K, int MV>
+__global__ void __launch_bounds__(256) k_rowgemm_reg(RowGemmArgs<T> a)
+{
+  __shared__ T sC[M * K];
+  __shared__ T sD[K * K];
+  for (int t = threadIdx.x; t < M * K; t += blockDim.x) {
+    const int i = t % M, j = t / M;
+    sC[t] = (i < a.m && j < a.k) ? a.C[i + j * a.ldc] : T(0);
+  }
+  if (a.mode == RM_VCWD)
+    for (int t = threadIdx.x; t < K * K; t += blockDim.x) {
+      const int i = t % K, j = t / K;
+      sD[t] = (i < a.k && j < a.k) ? a.D[i + j * a.ldd] : T(0);
+    }
+  __syncthreads();
+  constexpr int GM = (MV > K) ? MV : K;
+  T gacc[GM * K];
+#pragma unroll
+  for (int q = 0; q < GM * K; q++) gacc[q] = T(0);
+  for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < a.n;
+       i += (int64_t)gridDim.x * blockDim.x) {
+    T v[8], w[8], out[8];
+    if (a.mode == RM_MVSDI) load_row((const T*)a.W + i * a.ldw, a.m, M, v);
+    else load_row(a.V + i * a.ldv, a.m, M, v);
+    if (a.mode == RM_VCWD || (a.mode == RM_MVSD && a.beta != T(0)))
+      load_row((const T*)a.W + i * a.ldw, a.k, K, w);
+#pragma unroll
+    for (int q = 0; q < K; q++) {
+      T s = T(0);
+#pragma unroll
+      for (int p = 0; p < M; p++) s += v[p] * sC[p + q * M];
+      if (a.mode == RM_VCWD) {
+#pragma unroll
+        for (int p = 0; p < K; p++) s += w[p] * sD[p + q * K];
+      } else if (a.mode == RM_MVSD) {
+        s = (a.beta != T(0)) ? a.alpha * s + a.beta * w[q] : a.alpha * s;
+      }
+      out[q] = s;
+    }
+#pragma unroll
+    for (int q = 0; q < K; q++)
+      if (q < a.k) a.W[i * a.ldw + q] = out[q];
+    if (a.gram == GM_WW) {
+#pragma unroll
+      for (int q = 0; q < K; q++)
+#pragma unroll
+        for (int p = 0; p < K; p++) gacc[p + q * K] += out[p] * out[q];
+    } else if (a.gram == GM_VW) {
+      T g[8];
+      load_row(a.Vg + i * a.ldvg, a.mv, MV, g);
+#pragma unroll
+      for (int q = 0; q < K; q++)
+#pragma unroll
+        for (int p = 0; p < MV; p++) gacc[p + q * MV] += g[p] * out[q];
+    }
+  }
+  if (a.gram == GM_NONE) return;
+  const int gmax = (a.gram == GM_WW) ? K : MV;
+  // partial layout: gmax rows (padded), K columns
+  block_partial<T, GM * K>(gacc, a.part, gmax * K);
+  const T al = (a.gram == GM_WW) ? T(1) : a.galpha;
+  const T be = (a.gram == GM_WW) ? T(0) : a.gbeta;
+  last_block_reduce<T>(a.part, gmax * K, gridDim.x, a.counter, a.Gd, 1, gmax, a.ldg, al, be,
+                       (a.gram == GM_WW) ? a.k : a.mv, a.k);
 }
 
 }  // namespace pb

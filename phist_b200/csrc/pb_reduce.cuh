@@ -26,11 +26,14 @@ struct Acc<float> { typedef float type; };
 // the final reduction (its threads wrote out[o] = alpha*sum + beta*out[o],
 // with out[o] not read when beta == 0).  Output o goes to
 // out[(o % out_rows)*out_stride_rows + (o / out_rows)*ld_out].
+// Outputs whose row is >= vrows or whose column is >= vcols are padding and
+// are not written.
 template <class T>
 __device__ __forceinline__ bool last_block_reduce(const T* part, int nout, int nblocks,
                                                   unsigned int* counter, T* out,
                                                   int64_t out_stride_rows, int out_rows,
-                                                  int64_t ld_out, T alpha, T beta)
+                                                  int64_t ld_out, T alpha, T beta,
+                                                  int vrows = 1 << 30, int vcols = 1 << 30)
 {
   __shared__ bool am_last;
   __shared__ T red[256];  // all callers launch at most 256 threads per block
@@ -78,8 +81,10 @@ __device__ __forceinline__ bool last_block_reduce(const T* part, int nout, int n
     if (threadIdx.x < span) {
       const int o = o0 + threadIdx.x;
       const int r = o % out_rows, c = o / out_rows;
-      T* dst = out + r * out_stride_rows + (int64_t)c * ld_out;
-      *dst = (beta == T(0)) ? alpha * s : alpha * s + beta * (*dst);
+      if (r < vrows && c < vcols) {
+        T* dst = out + r * out_stride_rows + (int64_t)c * ld_out;
+        *dst = (beta == T(0)) ? alpha * s : alpha * s + beta * (*dst);
+      }
     }
   }
   if (threadIdx.x == 0) *counter = 0u;  // ready for the next launch

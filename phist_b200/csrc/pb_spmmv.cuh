@@ -133,7 +133,9 @@ constexpr int SPMV_BS = 256;
 // unrolled row loop); KMAX == 0: any length (runtime loop).
 // CC > 0: the chunk height is the compile-time constant CC (entry offsets
 // become immediates); CC == 0: read from A.C.
-template <class T, int NV, int TPR, bool VEC, int KMAX, int CC>
+// DOTS: the fused column dots are computed (bounded grid walking the row
+// tiles); otherwise one row tile per block and no dot code.
+template <class T, int NV, int TPR, bool VEC, int KMAX, int CC, bool DOTS>
 __global__ void __launch_bounds__(SPMV_BS)
 k_sell_spmmv(SellDev<T> A, SpmvArgs<T> p)
 {
@@ -146,11 +148,20 @@ k_sell_spmmv(SellDev<T> A, SpmvArgs<T> p)
 
   const int tid = threadIdx.x;
   const int s = tid % TPR;
-  const int64_t r = (int64_t)blockIdx.x * RPB + tid / TPR;  // SELL row
   const int C = CC > 0 ? CC : A.C;
-  const int64_t i = (r < A.nrows) ? (A.perm ? (int64_t)A.perm[r] : r) : -1;
   const int nv = p.nvec;
   const T* __restrict__ x = p.x + p.col0;
+  T wdw[VPT], vdw[VPT];  // column dot partials of this thread
+#pragma unroll
+  for (int q = 0; q < VPT; q++) { wdw[q] = T(0); vdw[q] = T(0); }
+
+  // tiles of RPB SELL rows; one tile per block unless the grid was bounded
+  // (fused dots: fewer blocks, fewer partial vectors to combine)
+  const int64_t ntiles = (A.nchunks * (int64_t)C + RPB - 1) / RPB;
+  const int64_t tstep = DOTS ? (int64_t)gridDim.x : ntiles;
+  for (int64_t tile = blockIdx.x; tile < ntiles; tile += tstep) {
+  const int64_t r = tile * RPB + tid / TPR;  // SELL row
+  const int64_t i = (r < A.nrows) ? (A.perm ? (int64_t)A.perm[r] : r) : -1;
 
   AT acc[VPT];
   T xi[VPT];
@@ -233,10 +244,6 @@ k_sell_spmmv(SellDev<T> A, SpmvArgs<T> p)
     }
   }
 
-  T wdw[VPT], vdw[VPT];
-#pragma unroll
-  for (int q = 0; q < VPT; q++) { wdw[q] = T(0); vdw[q] = T(0); }
-
   if (i >= 0) {
     T* yr = p.y + p.col0 + i * p.ldy;
 #pragma unroll
@@ -255,8 +262,10 @@ k_sell_spmmv(SellDev<T> A, SpmvArgs<T> p)
       Vec<T, VW>::st(yr + c, yv);
 #pragma unroll
       for (int w = 0; w < VW; w++) {
-        wdw[v * VW + w] = yv[w] * yv[w];
-        vdw[v * VW + w] = xi[v * VW + w] * yv[w];
+        if (DOTS) {
+          wdw[v * VW + w] += yv[w] * yv[w];
+          vdw[v * VW + w] += xi[v * VW + w] * yv[w];
+        }
       }
       if (p.u) {
         T* ur = p.u + p.col0 + i * p.ldu + c;
@@ -273,8 +282,9 @@ k_sell_spmmv(SellDev<T> A, SpmvArgs<T> p)
       }
     }
   }
+  }  // tiles
 
-  if (!(p.want_wdw || p.want_vdw)) return;
+  if (!DOTS) return;
 
   // ---- block reduction of the column dots, fixed order ----
   // lanes with equal s hold the same columns: butterfly over offsets >= TPR
