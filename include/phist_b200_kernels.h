@@ -373,6 +373,9 @@ void phist_b200_set_sell_params(int C, int64_t sigma, int* iflag);
  * 32:8|16) and, when unroll >= 0, whether the fully unrolled kernel for
  * matrices whose rows have at most 8 entries may be used */
 void phist_b200_set_spmv_config(int nvec, int tpr, int unroll, int* iflag);
+/* block widths >= min_nvec (8..32) use the SpMMV kernel that stages the
+ * gathered X rows in shared memory (values above 32 disable it) */
+void phist_b200_set_spmv_staged(int min_nvec, int* iflag);
 /* wait for all work this library enqueued */
 void phist_b200_synchronize(int* iflag);
 /* number of kernel launches this library has issued since init */

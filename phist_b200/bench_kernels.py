@@ -121,6 +121,19 @@ def suite_spmmv_tune(T, reps, peak, L=128):
     # back to the defaults
     for nv, tpr in ((4, 1), (8, 2), (16, 4), (32, 8)):
         K.chk(K.phist_b200_set_spmv_config, nv, tpr, 1)
+    # shared-memory staged kernel on / off for the wide widths
+    for nv in (8, 16, 32):
+        X = Mvec(A.domain_map, nv).set(random_block(n, nv, 3))
+        Y = Mvec(A.row_map, nv)
+        b = nnz * 12 + 16 * n * nv + (-(-n // 32)) * 12
+        for smin in (8, 99):
+            K.chk(K.phist_b200_set_spmv_staged, smin)
+            t = T.time(lambda: K.chk(K.phist_DsparseMat_times_mvec, 1.0, A.h, X.h, 0.0, Y.h), reps)
+            out.append(report("spmmv_staged%d" % (smin <= 32), {"n": n, "nnz": nnz, "nvec": nv},
+                              b, 2 * nnz * nv, t, peak))
+        X.delete()
+        Y.delete()
+    K.chk(K.phist_b200_set_spmv_staged, 8)
     A.delete()
     return out
 

@@ -12,8 +12,19 @@
 #include "pb_carp.cuh"
 #include "pb_core.hpp"
 #include "pb_spmmv.cuh"
+#include "pb_spmmv_staged.cuh"
+#include "pb_tile.cuh"
 
 namespace pb {
+
+// widths and leading dimensions in whole 16-byte vectors, 16-byte aligned start
+template <class T>
+inline bool vec_ok(const T* p, int64_t ld, int ncols)
+{
+  const int vw = 16 / (int)sizeof(T);
+  return (((uintptr_t)p) & 15u) == 0 && ld % vw == 0 && ncols % vw == 0;
+}
+inline int pad_width(int w) { return w <= 16 ? 16 : w <= 32 ? 32 : 64; }
 
 inline int grid_for(int64_t work, int bs = 256)
 {
@@ -584,6 +595,19 @@ void launch_spmv_nv(const SparseMat<T>* A, const SellDev<T>& S, SpmvArgs<T>& p, 
   }
   const bool fast = rt().spmv_unroll && A->C == 32 && A->max_row_len <= 8;
   const bool dots = p.want_wdw || p.want_vdw;
+  if constexpr (NV >= 8 && NV <= 32) {
+    // wide block vectors: X rows staged in shared memory by cp.async
+    if (fast && vec && !dots && !p.u && NV >= rt().spmv_staged_min_nvec) {
+      const size_t smem = StagedSmem<T, NV>::bytes;
+      const int bps = std::max(1, std::min(8, (int)((200 * 1024) / smem)));
+      const int sgrid = (int)std::min<int64_t>(A->nchunks > 0 ? A->nchunks : 1, (int64_t)rt().num_sms() * bps);
+      auto kern = k_sell_spmmv_staged<T, NV>;
+      PB_CUDA(cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+      kern<<<sgrid, 256, smem, stream()>>>(S, p);
+      PB_LAUNCH_CHECK();
+      return;
+    }
+  }
 #define PB_SPMV(VECv, KMAXv, CCv)                                                         \
   if (dots)                                                                             \
     k_sell_spmmv<T, NV, TPR, VECv, KMAXv, CCv, true><<<grid, SPMV_BS, 0, stream()>>>(S, p); \
@@ -758,6 +782,36 @@ void launch_mvTmv(int64_t n, int m, int k, T alpha, const T* V, int64_t ldv, con
     PB_LAUNCH_CHECK();
     return;
   }
+  if (m <= 64 && k <= 64 && vec_ok(V, ldv, m) && vec_ok(W, ldw, k)) {
+    // asynchronously staged tiles, widths padded to 16/32/64
+    const int BM = pad_width(m), BK = pad_width(k);
+    const int TT = (BM * BK >= 2048) ? 8 : 4;
+    constexpr int R = 64;
+    const int NT = (BM / TT) * (BK / TT), RG = BLK_BS / NT;
+    const size_t stage = sizeof(T) * 2 * R * (size_t)(BM + BK);
+    const size_t red = sizeof(T) * (size_t)RG * BM * BK;
+    const size_t smem = std::max(stage, red);
+    const int grid = (int)std::min<int64_t>(ceil_div(n > 0 ? n : 1, R), (int64_t)rt().num_sms() * (TT == 8 ? 1 : 2));
+    a.part = (T*)rt().scratch(sizeof(T) * (size_t)grid * m * k);
+    a.counter = rt().counters();
+    a.R = R;
+#define PB_MVA(BMv, BKv, TTv)                                                                  \
+  {                                                                                            \
+    auto kern = k_mvtmv_async<T, BMv, BKv, TTv, R>;                                            \
+    PB_CUDA(cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem)); \
+    kern<<<grid, BLK_BS, smem, stream()>>>(a);                                                 \
+  }
+    if (BM == 16) {
+      if (BK == 16) PB_MVA(16, 16, 4) else if (BK == 32) PB_MVA(16, 32, 4) else PB_MVA(16, 64, 4)
+    } else if (BM == 32) {
+      if (BK == 16) PB_MVA(32, 16, 4) else if (BK == 32) PB_MVA(32, 32, 4) else PB_MVA(32, 64, 8)
+    } else {
+      if (BK == 16) PB_MVA(64, 16, 4) else if (BK == 32) PB_MVA(64, 32, 8) else PB_MVA(64, 64, 8)
+    }
+#undef PB_MVA
+    PB_LAUNCH_CHECK();
+    return;
+  }
   const bool big = (int64_t)m * k >= 256;
   const int TM = big ? 8 : 4, TK = big ? 8 : 4;
   const int mp = ceil_div(m, TM) * TM, kp = ceil_div(k, TK) * TK;
@@ -810,6 +864,29 @@ void launch_rowgemm(RowGemmArgs<T>& a)
 #undef PB_RGR
     PB_LAUNCH_CHECK();
     return;
+  }
+  {
+    const T* A = (a.mode == RM_MVSDI) ? (const T*)a.W : a.V;
+    const int64_t lda = (a.mode == RM_MVSDI) ? a.ldw : a.ldv;
+    if (a.gram == GM_NONE && a.mode != RM_VCWD && a.m <= 64 && a.k <= 64 && vec_ok(A, lda, a.m)) {
+      // asynchronously staged row tiles of 64 rows, widths padded to 16/32/64
+      const int BM = pad_width(a.m), BK = pad_width(a.k);
+      const size_t smem = sizeof(T) * ((size_t)BM * BK + 2 * 64 * (size_t)(BM + 16 / sizeof(T)));
+      const int grid = (int)std::min<int64_t>(ceil_div(a.n > 0 ? a.n : 1, 64), (int64_t)rt().num_sms() * 2);
+#define PB_MSA(BMv, BKv, TRv)                                                                  \
+  {                                                                                            \
+    auto kern = k_mvsd_async<T, BMv, BKv, TRv, 4>;                                             \
+    PB_CUDA(cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem)); \
+    kern<<<grid, BLK_BS, smem, stream()>>>(a);                                                 \
+  }
+#define PB_MSA_K(BMv)                                                  \
+  if (BK == 16) PB_MSA(BMv, 16, 1) else if (BK == 32) PB_MSA(BMv, 32, 2) else PB_MSA(BMv, 64, 4)
+      if (BM == 16) { PB_MSA_K(16) } else if (BM == 32) { PB_MSA_K(32) } else { PB_MSA_K(64) }
+#undef PB_MSA_K
+#undef PB_MSA
+      PB_LAUNCH_CHECK();
+      return;
+    }
   }
   // micro-tile: TK columns per thread, TR rows
   const int TK = a.k >= 32 ? 8 : a.k >= 8 ? 4 : a.k >= 2 ? 2 : 1;

@@ -142,6 +142,8 @@ class Runtime {
   // and whether the fully unrolled short-row kernel may be used
   int spmv_tpr[6] = {1, 1, 1, 2, 4, 8};
   bool spmv_unroll = true;
+  // block widths >= this use the shared-memory staged kernel (> 32: never)
+  int spmv_staged_min_nvec = 8;
 
   // statistics: kernel launches issued by this library
   uint64_t launches = 0;

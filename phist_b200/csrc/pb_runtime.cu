@@ -439,6 +439,13 @@ void phist_b200_set_spmv_config(int nvec, int tpr, int unroll, int* iflag)
   PB_API_END(iflag);
 }
 
+void phist_b200_set_spmv_staged(int min_nvec, int* iflag)
+{
+  PB_API_BEGIN(iflag);
+  rt().spmv_staged_min_nvec = min_nvec;
+  PB_API_END(iflag);
+}
+
 void phist_b200_synchronize(int* iflag)
 {
   PB_API_BEGIN(iflag);

@@ -248,6 +248,37 @@ def test_rowfunc_matrix_equals_crs(session, oracle):
         X.delete(); Y.delete(); A.delete()
 
 
+@pytest.mark.parametrize("prob", ["ANDERSON3D-24-S1", "HONEYCOMB-40x24-S4", "LAPLACE3D-20"])
+@pytest.mark.parametrize("nvec", [8, 16, 32])
+def test_staged_kernel_matches_oracle_and_register_path(session, oracle, prob, nvec):
+    """short-row matrices at block widths 8..32 take the shared-memory staged
+    kernel; it must agree with the oracle and with the register kernel"""
+    from phist_b200 import generators as G
+    from phist_b200 import kernels as K
+    from phist_b200.objects import Mvec, SparseMat
+    K.chk(K.phist_b200_set_sell_params, 32, 256)
+    rp, c, v = G.problem(prob)
+    A = SparseMat.from_crs(rp, c, v, flags=K.PHIST_SPARSEMAT_PERM_LOCAL)
+    n = len(rp) - 1
+    x = G.random_block(n, nvec, 7)
+    y0 = G.random_block(n, nvec, 8)
+    sh = np.linspace(-1, 1, nvec)
+    X = Mvec(A.domain_map, nvec).set(x)
+    Y = Mvec(A.row_map, nvec)
+    outs = []
+    for staged_min in (8, 99):
+        K.chk(K.phist_b200_set_spmv_staged, staged_min)
+        Y.set(y0)
+        K.chk(K.phist_DsparseMat_times_mvec_vadd_mvec, 0.75, A.h, K.sptr(sh, np.float64), X.h, -0.5, Y.h)
+        outs.append(Y.get())
+    K.chk(K.phist_b200_set_spmv_staged, 8)
+    ref = oracle.spmmv(rp, c, v, x, alpha=0.75, beta=-0.5, y=y0, shifts=sh)
+    assert relerr(outs[0], ref) < TOL
+    assert relerr(outs[1], ref) < TOL
+    assert relerr(outs[0], outs[1]) < 1e-15
+    X.delete(); Y.delete(); A.delete()
+
+
 def test_read_mm(session, oracle, testmats, tmp_path):
     """sparseMat_read_mm (phist_kernels_decl.h:98) on a MatrixMarket file"""
     import ctypes as ct
