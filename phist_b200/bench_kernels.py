@@ -133,7 +133,7 @@ def suite_spmmv_tune(T, reps, peak, L=128):
                               b, 2 * nnz * nv, t, peak))
         X.delete()
         Y.delete()
-    K.chk(K.phist_b200_set_spmv_staged, 8)
+    K.chk(K.phist_b200_set_spmv_staged, 99)  # the library default
     A.delete()
     return out
 

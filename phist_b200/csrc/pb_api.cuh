@@ -26,6 +26,21 @@ inline bool vec_ok(const T* p, int64_t ld, int ncols)
 }
 inline int pad_width(int w) { return w <= 16 ? 16 : w <= 32 ? 32 : 64; }
 
+// raise a kernel's dynamic shared-memory limit once (the attribute call is a
+// host round trip that would otherwise precede every launch)
+template <class K>
+inline void set_smem(K kern, size_t smem)
+{
+  static std::mutex mu;
+  static std::map<const void*, size_t> done;
+  std::lock_guard<std::mutex> g(mu);
+  size_t& have = done[(const void*)kern];
+  if (smem > have) {
+    PB_CUDA(cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+    have = smem;
+  }
+}
+
 inline int grid_for(int64_t work, int bs = 256)
 {
   int64_t g = ceil_div(work > 0 ? work : 1, bs);
@@ -132,6 +147,34 @@ void copy_cols(const Mvec<T>* X, int xoff, Mvec<T>* Y, int yoff, int ncols)
   PB_LAUNCH_CHECK();
 }
 
+// V(:,j) *= s[j] with the host coefficients passed by value (64 columns per launch)
+template <class T>
+void vscale_cols(Mvec<T>* V, const T* s)
+{
+  if (V->nrows == 0) return;
+  for (int c0 = 0; c0 < V->nvec; c0 += 64) {
+    const int nv = std::min(64, V->nvec - c0);
+    Coef64<T> c;
+    for (int j = 0; j < nv; j++) c.v[j] = s[c0 + j];
+    k_vscale_v<T><<<grid_for((int64_t)V->nrows * nv), 256, 0, stream()>>>(V->d() + c0, V->lda, V->nrows, nv, c);
+    PB_LAUNCH_CHECK();
+  }
+}
+
+// Y(:,j) = alpha[j] X(:,j) + beta Y(:,j), coefficients passed by value
+template <class T>
+void vadd_cols(const T* alpha, const Mvec<T>* X, T beta, Mvec<T>* Y)
+{
+  if (Y->nrows == 0) return;
+  for (int c0 = 0; c0 < Y->nvec; c0 += 64) {
+    const int nv = std::min(64, Y->nvec - c0);
+    Coef64<T> c;
+    for (int j = 0; j < nv; j++) c.v[j] = alpha[c0 + j];
+    k_axpby_v<T><<<grid_for((int64_t)Y->nrows * nv), 256, 0, stream()>>>(X->d() + c0, X->lda, Y->d() + c0, Y->lda, Y->nrows, nv, c, beta);
+    PB_LAUNCH_CHECK();
+  }
+}
+
 template <class T>
 void check_same_rows(const Mvec<T>* a, const Mvec<T>* b)
 {
@@ -145,9 +188,9 @@ void mvec_upload(Mvec<T>* V)
 {
   if (V->nrows == 0) return;
   T* h = V->h();
+  // the host mirror is pageable: staged before the call returns (see sd_upload)
   PB_CUDA(cudaMemcpy2DAsync(V->d(), V->lda * sizeof(T), h, V->lda * sizeof(T),
                             V->nvec * sizeof(T), V->nrows, cudaMemcpyHostToDevice, stream()));
-  rt().sync();
 }
 template <class T>
 void mvec_download(Mvec<T>* V)
@@ -241,13 +284,15 @@ void sdmat_delete(void* vM)
   delete s;
 }
 
+// The host copy of an sdMat is pageable memory: cudaMemcpy*Async stages it
+// before returning, so the host copy may change right after this call and no
+// stream drain is needed (the device copy is updated in stream order).
 template <class T>
 void sd_upload(SdMat<T>* M)
 {
   if (M->nrows == 0 || M->ncols == 0) return;
   PB_CUDA(cudaMemcpy2DAsync(M->d(), M->lda * sizeof(T), M->h(), M->lda * sizeof(T),
                             M->nrows * sizeof(T), M->ncols, cudaMemcpyHostToDevice, stream()));
-  rt().sync();
 }
 template <class T>
 void sd_download(SdMat<T>* M)
@@ -602,7 +647,7 @@ void launch_spmv_nv(const SparseMat<T>* A, const SellDev<T>& S, SpmvArgs<T>& p, 
       const int bps = std::max(1, std::min(8, (int)((200 * 1024) / smem)));
       const int sgrid = (int)std::min<int64_t>(A->nchunks > 0 ? A->nchunks : 1, (int64_t)rt().num_sms() * bps);
       auto kern = k_sell_spmmv_staged<T, NV>;
-      PB_CUDA(cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+      set_smem(kern, smem);
       kern<<<sgrid, 256, smem, stream()>>>(S, p);
       PB_LAUNCH_CHECK();
       return;
@@ -798,7 +843,7 @@ void launch_mvTmv(int64_t n, int m, int k, T alpha, const T* V, int64_t ldv, con
 #define PB_MVA(BMv, BKv, TTv)                                                                  \
   {                                                                                            \
     auto kern = k_mvtmv_async<T, BMv, BKv, TTv, R>;                                            \
-    PB_CUDA(cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem)); \
+    set_smem(kern, smem); \
     kern<<<grid, BLK_BS, smem, stream()>>>(a);                                                 \
   }
     if (BM == 16) {
@@ -829,11 +874,11 @@ void launch_mvTmv(int64_t n, int m, int k, T alpha, const T* V, int64_t ldv, con
   a.counter = rt().counters();
   if (big) {
     auto kern = k_mvTmv<T, 8, 8>;
-    PB_CUDA(cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+    set_smem(kern, smem);
     kern<<<grid, BLK_BS, smem, stream()>>>(a);
   } else {
     auto kern = k_mvTmv<T, 4, 4>;
-    PB_CUDA(cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+    set_smem(kern, smem);
     kern<<<grid, BLK_BS, smem, stream()>>>(a);
   }
   PB_LAUNCH_CHECK();
@@ -868,7 +913,9 @@ void launch_rowgemm(RowGemmArgs<T>& a)
   {
     const T* A = (a.mode == RM_MVSDI) ? (const T*)a.W : a.V;
     const int64_t lda = (a.mode == RM_MVSDI) ? a.ldw : a.ldv;
-    if (a.gram == GM_NONE && a.mode != RM_VCWD && a.m <= 64 && a.k <= 64 && vec_ok(A, lda, a.m)) {
+    const bool gram_ok = a.gram == GM_NONE || (vec_ok((const T*)a.W, a.ldw, a.k) &&
+                                               (a.gram == GM_WW || (a.mv <= 64 && vec_ok(a.Vg, a.ldvg, a.mv))));
+    if (gram_ok && a.mode != RM_VCWD && a.m <= 64 && a.k <= 64 && vec_ok(A, lda, a.m)) {
       // asynchronously staged row tiles of 64 rows, widths padded to 16/32/64
       const int BM = pad_width(a.m), BK = pad_width(a.k);
       const size_t smem = sizeof(T) * ((size_t)BM * BK + 2 * 64 * (size_t)(BM + 16 / sizeof(T)));
@@ -876,7 +923,7 @@ void launch_rowgemm(RowGemmArgs<T>& a)
 #define PB_MSA(BMv, BKv, TRv)                                                                  \
   {                                                                                            \
     auto kern = k_mvsd_async<T, BMv, BKv, TRv, 4>;                                             \
-    PB_CUDA(cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem)); \
+    set_smem(kern, smem); \
     kern<<<grid, BLK_BS, smem, stream()>>>(a);                                                 \
   }
 #define PB_MSA_K(BMv)                                                  \
@@ -885,6 +932,12 @@ void launch_rowgemm(RowGemmArgs<T>& a)
 #undef PB_MSA_K
 #undef PB_MSA
       PB_LAUNCH_CHECK();
+      // fused Gram at these widths: a second pass over the new W with the
+      // staged Gram kernel (the register kernels above fuse it into one pass)
+      if (a.gram == GM_WW)
+        launch_mvTmv<T>(a.n, a.k, a.k, T(1), a.W, a.ldw, a.W, a.ldw, T(0), a.Gd, a.ldg);
+      else if (a.gram == GM_VW)
+        launch_mvTmv<T>(a.n, a.mv, a.k, a.galpha, a.Vg, a.ldvg, a.W, a.ldw, a.gbeta, a.Gd, a.ldg);
       return;
     }
   }
@@ -913,7 +966,7 @@ void launch_rowgemm(RowGemmArgs<T>& a)
 #define PB_RG_LAUNCH(TRv, TKv)                                                                 \
   {                                                                                            \
     auto kern = k_rowgemm<T, TRv, TKv>;                                                        \
-    PB_CUDA(cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem)); \
+    set_smem(kern, smem); \
     kern<<<grid, BLK_BS, smem, stream()>>>(a);                                                 \
   }
   if (TK == 8) PB_RG_LAUNCH(4, 8)
@@ -1041,14 +1094,16 @@ void carp_run(const CarpWork<T>* w, int nvec, const T* sr, const T* si, const Mv
       a.q1 = w->h_color_ptr[color + 1];
       const int64_t cnt = a.q1 - a.q0;
       if (cnt <= 0) return;
-      const int grid = (int)ceil_div(cnt, 256);
-#define PB_KZ(NVv)                                                       \
-  k_kacz_color<T, NVv, RC><<<grid, 256, 0, stream()>>>(a);
-      if (nv <= 1) PB_KZ(1)
-      else if (nv <= 2) PB_KZ(2)
-      else if (nv <= 4) PB_KZ(4)
-      else if (nv <= 8) PB_KZ(8)
-      else if (nv <= 16) PB_KZ(16)
+      // one thread per (row, column): TPR = nv rounded up to a power of two
+      const int TPR = nv <= 1 ? 1 : nv <= 2 ? 2 : nv <= 4 ? 4 : nv <= 8 ? 8 : nv <= 16 ? 16 : 32;
+      const int grid = (int)ceil_div(cnt * TPR, 256);
+#define PB_KZ(TPRv)                                                       \
+  k_kacz_color_cols<T, TPRv, RC><<<grid, 256, 0, stream()>>>(a);
+      if (TPR == 1) PB_KZ(1)
+      else if (TPR == 2) PB_KZ(2)
+      else if (TPR == 4) PB_KZ(4)
+      else if (TPR == 8) PB_KZ(8)
+      else if (TPR == 16) PB_KZ(16)
       else PB_KZ(32)
 #undef PB_KZ
       PB_LAUNCH_CHECK();

@@ -62,6 +62,30 @@ __global__ void k_axpby(const T* __restrict__ x, int64_t ldx, T* y, int64_t ldy,
   }
 }
 
+// per-column coefficients passed by value (no host-to-device copy)
+template <class T>
+struct Coef64 {
+  T v[64];
+};
+
+template <class T>
+__global__ void k_axpby_v(const T* __restrict__ x, int64_t ldx, T* y, int64_t ldy, int64_t n,
+                          int nvec, Coef64<T> alpha, T beta)
+{
+  PB_FOR_ELEMS(n, nvec, i, j)
+  {
+    const T a = alpha.v[j];
+    const T xv = (a == T(0)) ? T(0) : a * x[i * ldx + j];
+    y[i * ldy + j] = (beta == T(0)) ? xv : xv + beta * y[i * ldy + j];
+  }
+}
+
+template <class T>
+__global__ void k_vscale_v(T* v, int64_t ld, int64_t n, int nvec, Coef64<T> s)
+{
+  PB_FOR_ELEMS(n, nvec, i, j) v[i * ld + j] *= s.v[j];
+}
+
 // W(i,j) = alpha * V(i, bc ? 0 : j) * W(i,j)
 template <class T>
 __global__ void k_elemwise(const T* __restrict__ v, int64_t ldv, T* w, int64_t ldw, int64_t n,

@@ -115,6 +115,62 @@ __global__ void __launch_bounds__(256) k_kacz_color(KaczArgs<T> a)
   }
 }
 
+// One thread per (row, column): TPR consecutive threads (TPR >= nvec, a power
+// of two) share a row, thread j owns column j.  Within a colour class the
+// (row, column) projections are independent of each other (distance-2
+// colouring, and columns never mix), so no thread waits for another; the
+// TPR threads of a row read and write each X row as one contiguous segment.
+template <class T, int TPR, bool RC>
+__global__ void __launch_bounds__(256) k_kacz_color_cols(KaczArgs<T> a)
+{
+  const int64_t q = a.q0 + (blockIdx.x * (int64_t)blockDim.x + threadIdx.x) / TPR;
+  const int j = threadIdx.x % TPR;
+  if (q >= a.q1 || j >= a.nvec) return;
+  const int64_t i = a.rows[q];
+  const int64_t p0 = a.rp[q], p1 = a.rp[q + 1];
+  const T sr = a.sig_r[j];
+  const T si = RC ? a.sig_i[j] : T(0);
+  T tr, ti = T(0);
+  {
+    const T xr = a.xr[i * a.ldxr + j];
+    if (RC) {
+      const T xi = a.xi[i * a.ldxi + j];
+      tr = -sr * xr + si * xi;
+      ti = -si * xr - sr * xi;
+    } else {
+      tr = -sr * xr;
+    }
+  }
+#pragma unroll 4
+  for (int64_t p = p0; p < p1; p++) {
+    const T v = a.val[p];
+    const int64_t c = a.col[p];
+    tr += v * a.xr[c * a.ldxr + j];
+    if (RC) ti += v * a.xi[c * a.ldxi + j];
+  }
+  if (a.b) tr -= a.b[i * a.ldb + j];
+  const T nrm = a.nrm[q], d = a.diag[q];
+  T rn = nrm - T(2) * d * sr + sr * sr;
+  if (RC) rn += si * si;
+  if (rn == T(0)) rn = T(1);
+  const T f = a.omega[j] / rn;
+  tr *= f;
+  if (RC) {
+    ti *= f;
+    a.xr[i * a.ldxr + j] += tr * sr + ti * si;
+    a.xi[i * a.ldxi + j] += ti * sr - tr * si;
+  } else {
+    a.xr[i * a.ldxr + j] += tr * sr;
+  }
+#pragma unroll 4
+  for (int64_t p = p0; p < p1; p++) {
+    const T v = a.val[p];
+    const int64_t c = a.col[p];
+    a.xr[c * a.ldxr + j] -= tr * v;
+    if (RC) a.xi[c * a.ldxi + j] -= ti * v;
+  }
+}
+
 // Greedy distance-2 colouring in natural row order: row i takes the smallest
 // colour not used by any row that shares a column with it.  colT is the
 // column -> rows pattern (transpose).

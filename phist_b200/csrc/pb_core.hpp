@@ -142,8 +142,11 @@ class Runtime {
   // and whether the fully unrolled short-row kernel may be used
   int spmv_tpr[6] = {1, 1, 1, 2, 4, 8};
   bool spmv_unroll = true;
-  // block widths >= this use the shared-memory staged kernel (> 32: never)
-  int spmv_staged_min_nvec = 8;
+  // block widths >= this use the shared-memory staged kernel (> 32: never).
+  // Off by default: with one chunk per pipeline stage it measured slower
+  // than the register kernel on the 3D Anderson matrix (nvec 8/16/32:
+  // 219/436/1077 us against 152/285/545 us).
+  int spmv_staged_min_nvec = 99;
 
   // statistics: kernel launches issued by this library
   uint64_t launches = 0;
