@@ -31,10 +31,6 @@ def build(with_ref=None):
         targets.append("ref")
     env = dict(os.environ, PHIST_SRC=src)
     subprocess.run(["make", "-s", "-C", HERE] + targets, check=True, env=env)
-    if with_ref:
-        # PHIST's solver layers against the b200 library (needs the library built)
-        subprocess.run(["make", "-s", "-j8", "-C", os.path.join(HERE, "solvers"),
-                        "CXX_=g++", "CC_=gcc"], check=True, env=env)
 
 
 _lib = None

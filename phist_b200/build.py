@@ -6,6 +6,11 @@ The CUDA sources under phist_b200/csrc/ are compiled for sm_100a only and
 linked into one shared library, phist_b200/lib/libphist_kernels_b200.so,
 whose exported symbols are the C ABI declared in include/phist_b200_kernels.h.
 Object files are rebuilt only when a source or header is newer.
+
+build_solvers() then compiles PHIST's unchanged solver layers against that
+library, together with this package's FP32 correction solver and the drivers
+(phist_b200/solvers/Makefile), when the PHIST sources are reachable
+(PHIST_SRC); without them the prebuilt outputs in phist_b200/lib are used.
 """
 import os
 import subprocess
@@ -71,6 +76,21 @@ def build(verbose=False):
     return LIBPATH
 
 
+def build_solvers(verbose=False):
+    """make -C phist_b200/solvers (PHIST solver layers + drivers), if the
+    PHIST sources are present; returns True when they were built"""
+    src = os.environ.get("PHIST_SRC", "/root/reference")
+    if not os.path.isdir(os.path.join(src, "src", "jada")):
+        return False
+    env = dict(os.environ, PHIST_SRC=src)
+    subprocess.run(["make", "-s", "-j8", "-C", os.path.join(HERE, "solvers"), "CXX_=g++", "CC_=gcc"],
+                   check=True, env=env)
+    if verbose:
+        print("built PHIST solver layers into", LIBDIR)
+    return True
+
+
 if __name__ == "__main__":
     build(verbose=True)
+    build_solvers(verbose=True)
     sys.exit(0)

@@ -14,6 +14,9 @@
 //         maxIters innerSolvType(GMRES|MINRES) innerSolvMaxIters symmetry(GENERAL|HERMITIAN)
 //         seed (start block uniform[-1,1) from this seed) sigma (SELL sigma)
 //         reps (repeat the solve, report each wall time)
+//         mixed=1 (FP32 correction equations through pb_mixed_jada.h; the
+//         outer iteration, Rayleigh-Ritz, orthogonalisation and residuals
+//         stay FP64)
 #include <chrono>
 #include <cmath>
 #include <cstdio>
@@ -27,6 +30,7 @@
 #include "phist_core.h"
 #include "phist_jada.h"
 #include "phist_enums.h"
+#include "pb_mixed_jada.h"
 
 extern "C" {
 void phist_b200_Dcreate_problem(phist_DsparseMat_ptr* A, phist_const_comm_ptr comm,
@@ -84,6 +88,7 @@ int main(int argc, char** argv)
   uint64_t seed = 0;
   int64_t sigma = 1;
   int reps = 1;
+  int mixed = 0;
   for (int a = 2; a < argc; a++) {
     const char* kv = argv[a];
     const char* eq = strchr(kv, '=');
@@ -104,6 +109,7 @@ int main(int argc, char** argv)
     else if (k == "seed") seed = strtoull(v, nullptr, 10);
     else if (k == "sigma") sigma = atoll(v);
     else if (k == "reps") reps = atoi(v);
+    else if (k == "mixed") mixed = atoi(v);
   }
 
   CHK(phist_kernels_init(&argc, &argv, &iflag));
@@ -123,6 +129,12 @@ int main(int argc, char** argv)
   CHK(phist_DsparseMat_get_domain_map(A, &map, &iflag));
   phist_lidx nloc = 0;
   CHK(phist_map_get_local_length(map, &nloc, &iflag));
+
+  pb_mixed_jada* mixedSolver = NULL;
+  if (mixed) {
+    CHK(phist_b200_mixed_jada_create(&mixedSolver, A, &opts, &iflag));
+    CHK(phist_b200_mixed_jada_install(mixedSolver, &opts, &iflag));
+  }
 
   const int nEig = opts.numEigs, bs = opts.blockSize;
   const int nQ = nEig + bs - 1;
@@ -179,10 +191,13 @@ int main(int argc, char** argv)
     CHK(phist_Dmvec_delete(Q, &iflag));
     CHK(phist_DsdMat_delete(R, &iflag));
   }
-  printf("{\"problem\": \"%s\", \"n\": %d, \"numEigs\": %d, \"blockSize\": %d, \"minBas\": %d, "
+  long mcalls = 0, msys = 0, munconv = 0;
+  if (mixedSolver) CHK(phist_b200_mixed_jada_stats(mixedSolver, &mcalls, &msys, &munconv, &iflag));
+  printf("{\"problem\": \"%s\", \"mixed\": %d, \"inner_calls\": %ld, \"inner_systems\": %ld, "
+         "\"inner_unconverged\": %ld, \"n\": %d, \"numEigs\": %d, \"blockSize\": %d, \"minBas\": %d, "
          "\"maxBas\": %d, \"convTol\": %.3e, \"nConv\": %d, \"nIter\": %d, \"t_create\": %.4f, "
          "\"launches\": %llu, \"wall\": [",
-         problem, nloc, nEig, bs, opts.minBas, opts.maxBas, opts.convTol, nConv, nIter, t_create,
+         problem, mixed, mcalls, msys, munconv, nloc, nEig, bs, opts.minBas, opts.maxBas, opts.convTol, nConv, nIter, t_create,
          (unsigned long long)launches);
   for (size_t i = 0; i < walls.size(); i++) printf("%s%.6f", i ? ", " : "", walls[i]);
   printf("], \"ev\": [");
@@ -193,6 +208,7 @@ int main(int argc, char** argv)
   for (size_t i = 0; i < resx_out.size(); i++) printf("%s%.6e", i ? ", " : "", resx_out[i]);
   printf("]}\n");
   fflush(stdout);
+  if (mixedSolver) CHK(phist_b200_mixed_jada_delete(mixedSolver, &iflag));
   CHK(phist_DsparseMat_delete(A, &iflag));
   CHK(phist_comm_delete(comm, &iflag));
   CHK(phist_kernels_finalize(&iflag));

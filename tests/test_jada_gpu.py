@@ -1,7 +1,8 @@
 """PHIST's own block Jacobi-Davidson (subspacejada), compiled unchanged from
-the PHIST sources into oracle/_ref/ (oracle/solvers/Makefile), running on the
-b200 kernel library: the drop-in boundary exercised by the reference's own
-caller.  Checked against the closed-form spectrum of the Dirichlet 7-point
+the PHIST sources into phist_b200/lib/ (phist_b200/solvers/Makefile), running
+on the b200 kernel library: the drop-in boundary exercised by the reference's
+own caller, in FP64 and in the mixed form (FP32 correction equations through
+PHIST's user-defined inner-solver hook, pb_mixed_jada.h).  Checked against the closed-form spectrum of the Dirichlet 7-point
 Laplacian on L^3: lambda = sum_d (2 - 2 cos(k_d pi / (L+1))), k_d = 1..L.
 The reference's JaDa test accepts residuals below 20*tol
 (test/jada/TestSubspaceJaDa_def.hpp:167); eigenvalues must match to 1e-10
@@ -16,7 +17,7 @@ import pytest
 from conftest import ROOT
 
 pytestmark = pytest.mark.gpu
-RUNNER = os.path.join(ROOT, "oracle", "_ref", "jada_run")
+RUNNER = os.path.join(ROOT, "phist_b200", "lib", "jada_run")
 
 
 def laplace_eigs(L, k):
@@ -27,7 +28,7 @@ def laplace_eigs(L, k):
 
 def run(problem, *kv, timeout=600):
     if not os.path.exists(RUNNER):
-        pytest.skip("PHIST solver layers not built (oracle/solvers/Makefile)")
+        pytest.skip("PHIST solver layers not built (phist_b200/solvers/Makefile)")
     out = subprocess.run([RUNNER, problem] + list(kv), capture_output=True, text=True, timeout=timeout)
     assert out.returncode == 0, out.stderr[-2000:]
     line = [l for l in out.stdout.splitlines() if l.startswith("{")][-1]
@@ -69,3 +70,53 @@ def test_subspacejada_config1_laplace64(session):
     assert r["nConv"] >= 10
     check_spectrum(r["ev"][:10], 64, 10, tol)
     assert max(r["resExplicit"][:10]) < 20 * tol
+
+
+@pytest.mark.parametrize("L", [12, 16])
+def test_subspacejada_mixed_laplace_small(session, L):
+    """FP32 correction equations, FP64 outer iteration: the same eigenpairs
+    to the same tolerance as the all-FP64 run, within a few more outer
+    iterations"""
+    tol = 1e-10
+    args = ["LAPLACE3D-%d" % L, "numEigs=10", "blockSize=4", "minBas=20", "maxBas=40",
+            "convTol=%g" % tol, "which=SR"]
+    r64 = run(*args)
+    r32 = run(*(args + ["mixed=1"]))
+    assert r32["mixed"] == 1 and r32["inner_calls"] > 0
+    assert r32["nConv"] >= 10
+    check_spectrum(r32["ev"][:10], L, 10, tol)
+    assert max(r32["resExplicit"][:10]) < 20 * tol
+    # same converged eigenvalues as the FP64 run, to tol relative to the spectral radius
+    assert np.abs(np.sort(r32["ev"][:10]) - np.sort(r64["ev"][:10])).max() <= tol * 12.0
+    assert r32["nIter"] <= 1.5 * r64["nIter"] + 5
+
+
+def anderson_interior(L, seed, k):
+    """the k eigenvalues nearest 0 of the periodic Anderson matrix (dense
+    eigvalsh of the generator's CRS arrays)"""
+    from phist_b200.generators import anderson3d
+    rp, c, v = anderson3d(L, seed)
+    n = len(rp) - 1
+    A = np.zeros((n, n))
+    for i in range(n):
+        A[i, c[rp[i]:rp[i + 1]]] += v[rp[i]:rp[i + 1]]
+    ev = np.linalg.eigvalsh(A)
+    return ev[np.argsort(np.abs(ev))[:k]], np.abs(ev).max()
+
+
+@pytest.mark.parametrize("mixed", [0, 1])
+def test_subspacejada_anderson_interior(session, mixed):
+    """eigenvalues nearest 0 (which=SM) of a 3D Anderson matrix, L=10, block
+    size 8: every converged Ritz value is an exact eigenvalue (dense
+    eigvalsh) and lies among the eigenvalues nearest 0"""
+    tol = 1e-10
+    nev = 8
+    r = run("ANDERSON3D-10-S3", "numEigs=%d" % nev, "blockSize=8", "minBas=24", "maxBas=48",
+            "convTol=%g" % tol, "which=SM", "symmetry=HERMITIAN", "seed=3", "maxIters=400",
+            "mixed=%d" % mixed)
+    assert r["nConv"] >= nev
+    near, rho = anderson_interior(10, 3, 3 * nev)
+    ev = np.asarray(r["ev"][:nev])
+    for lam in ev:
+        assert np.abs(near - lam).min() <= tol * rho, (lam, near)
+    assert max(r["resExplicit"][:nev]) < 20 * tol
