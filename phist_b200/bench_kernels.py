@@ -152,6 +152,11 @@ def suite_block(T, reps, peak, n=1 << 21):
         G = SdMat(k, k)
         t = T.time(lambda: K.chk(K.phist_DmvecT_times_mvec, 1.0, V.h, W.h, 0.0, C.h), reps)
         out.append(report("mvecT_times_mvec", {"n": n, "m": m, "k": k}, 8 * n * (m + k), 2 * n * m * k, t, peak))
+        # the same product with the result left on the device (no download, no host sync)
+        t = T.time(lambda: K.chk(K.phist_DmvecT_times_mvec, 1.0, V.h, W.h, 0.0, C.h,
+                                 flags=K.PHIST_SDMAT_RUN_ON_DEVICE), reps)
+        out.append(report("mvecT_times_mvec_device", {"n": n, "m": m, "k": k}, 8 * n * (m + k), 2 * n * m * k,
+                          t, peak))
         t = T.time(lambda: K.chk(K.phist_Dmvec_times_sdMat, 1.0, V.h, C.h, 0.0, W.h), reps)
         out.append(report("mvec_times_sdMat", {"n": n, "m": m, "k": k}, 8 * n * (m + k), 2 * n * m * k, t, peak))
         t = T.time(lambda: K.chk(K.phist_Dmvec_times_sdMat_inplace, W.h, C.h), reps)
@@ -182,6 +187,56 @@ def suite_blas(T, reps, peak, n=1 << 21):
         X.delete()
         Y.delete()
     m_.delete()
+    return out
+
+
+def suite_latency(T, reps, peak, n=262144):
+    """host wall time per call, as a solver sees it, at the size of the 64^3
+    Laplacian (no L2 flush; the median of 200 back-to-back calls)"""
+    import time
+
+    from . import kernels as K
+    from .generators import random_block
+    from .objects import Map, Mvec, SdMat, SparseMat, sync
+    A = SparseMat.from_problem("LAPLACE3D-64")
+    m_ = A.domain_map
+    X1 = Mvec(m_, 1).set(random_block(n, 1, 1))
+    Y1 = Mvec(m_, 1).set(random_block(n, 1, 2))
+    X4 = Mvec(m_, 4).set(random_block(n, 4, 3))
+    Y4 = Mvec(m_, 4).set(random_block(n, 4, 4))
+    V = Mvec(m_, 40).set(random_block(n, 40, 5))
+    C = SdMat(40, 4)
+    C44 = SdMat(4, 4).set(np.eye(4))
+    d = np.zeros(4)
+    a4 = np.array([0.5, -0.25, 1.0, 2.0])
+    calls = {
+        "mvec_dot_mvec_nvec1": lambda: K.chk(K.phist_Dmvec_dot_mvec, X1.h, Y1.h, K.sptr(d, np.float64)),
+        "mvec_dot_mvec_nvec4": lambda: K.chk(K.phist_Dmvec_dot_mvec, X4.h, Y4.h, K.sptr(d, np.float64)),
+        "mvec_norm2_nvec4": lambda: K.chk(K.phist_Dmvec_norm2, X4.h, K.sptr(d, np.float64)),
+        "mvec_vadd_mvec_nvec4": lambda: K.chk(K.phist_Dmvec_vadd_mvec, K.sptr(a4, np.float64), X4.h, 1.0, Y4.h),
+        "mvec_add_mvec_nvec1": lambda: K.chk(K.phist_Dmvec_add_mvec, 0.5, X1.h, 1.0, Y1.h),
+        "spmmv_nvec4": lambda: K.chk(K.phist_DsparseMat_times_mvec, 1.0, A.h, X4.h, 0.0, Y4.h),
+        "mvecT_times_mvec_40x4": lambda: K.chk(K.phist_DmvecT_times_mvec, 1.0, V.h, X4.h, 0.0, C.h),
+        "mvec_times_sdMat_40x4": lambda: K.chk(K.phist_Dmvec_times_sdMat, 1.0, V.h, C.h, 0.0, Y4.h),
+        "mvec_times_sdMat_inplace_4x4": lambda: K.chk(K.phist_Dmvec_times_sdMat_inplace, Y4.h, C44.h),
+    }
+    out = []
+    for name, f in calls.items():
+        for _ in range(20):
+            f()
+        sync()
+        ts = []
+        for _ in range(200):
+            t0 = time.perf_counter()
+            f()
+            ts.append(time.perf_counter() - t0)
+        sync()
+        line = {"kernel": name, "n": n, "host_us_p50": round(float(np.median(ts)) * 1e6, 2),
+                "host_us_p90": round(float(np.percentile(ts, 90)) * 1e6, 2)}
+        print(json.dumps(line), flush=True)
+        out.append(line)
+    for o in (X1, Y1, X4, Y4, V, C, C44, A):
+        o.delete()
     return out
 
 
