@@ -15,6 +15,9 @@
 //   keys: nshifts (32) block (8) tol (1e-10) maxIter (20000) seed (4)
 //         omega (1.0) sigma (SELL sigma, 1) reps (1)
 //         out (file receiving the solutions X, n x nshifts row-major float64)
+//         mixed=1: FP32 CARP-CG inside FP64 iterative refinement
+//         (pb_mixed_carp.h) with innerTol (1e-5) and maxRefine (20); maxIter
+//         then bounds the FP32 iterations of each refinement step
 //   shifts sigma_j = 2.5 * u(seed, j), right-hand sides b_ij = u(seed + 1 + j, i)
 //   with u uniform [-1,1) from a splitmix64 hash (the library's pb_unif).
 #include <algorithm>
@@ -31,6 +34,7 @@
 #include "phist_core.h"
 #include "phist_krylov.h"
 #include "phist_enums.h"
+#include "pb_mixed_carp.h"
 
 extern "C" {
 void phist_b200_Dcreate_problem(phist_DsparseMat_ptr* A, phist_const_comm_ptr comm,
@@ -76,6 +80,8 @@ int main(int argc, char** argv)
   uint64_t seed = 4;
   int64_t sigma = 1;
   std::string out;
+  int mixed = 0, maxRefine = 20;
+  double innerTol = 1e-5;
   for (int a = 2; a < argc; a++) {
     const char* kv = argv[a];
     const char* eq = strchr(kv, '=');
@@ -91,6 +97,9 @@ int main(int argc, char** argv)
     else if (k == "sigma") sigma = atoll(v);
     else if (k == "reps") reps = atoi(v);
     else if (k == "out") out = v;
+    else if (k == "mixed") mixed = atoi(v);
+    else if (k == "innerTol") innerTol = atof(v);
+    else if (k == "maxRefine") maxRefine = atoi(v);
   }
   if (block < 1 || nshifts < 1) return 2;
 
@@ -121,11 +130,12 @@ int main(int argc, char** argv)
   }
 
   std::vector<double> walls, relres(nshifts, 0.0);
-  std::vector<int> iters, conv(nshifts, 0);
+  std::vector<int> iters, refines, conv(nshifts, 0);
   uint64_t launches = 0;
   for (int rep = 0; rep < reps; rep++) {
     CHK(phist_Dmvec_put_value(X, 0.0, &iflag));
     iters.clear();
+    refines.clear();
     uint64_t l0 = 0, l1 = 0;
     CHK(phist_b200_launch_count(&l0, &iflag));
     CHK(phist_b200_synchronize(&iflag));
@@ -135,19 +145,35 @@ int main(int argc, char** argv)
       phist_Dmvec_ptr Bj = NULL, Xj = NULL;
       CHK(phist_Dmvec_view_block(B, &Bj, j0, j0 + w - 1, &iflag));
       CHK(phist_Dmvec_view_block(X, &Xj, j0, j0 + w - 1, &iflag));
-      phist_Dcarp_cgState_ptr S = NULL;
-      CHK(phist_Dcarp_cgState_create(&S, A, NULL, w, &shifts[j0], NULL, &iflag));
-      for (int j = 0; j < w; j++) S->omega_[j] = omega;
-      CHK(phist_Dcarp_cgState_reset(S, Bj, NULL, &iflag));
-      iflag = 0;
-      phist_Dcarp_cgState_iterate(S, Xj, NULL, tol, maxIter, 0, &iflag);
-      if (iflag < 0) {
-        fprintf(stderr, "carp_cgState_iterate returned %d\n", iflag);
-        return 1;
+      if (mixed) {
+        pb_mixed_carp* M = NULL;
+        std::vector<double> om(w, omega);
+        CHK(phist_b200_mixed_carp_create(&M, A, w, &shifts[j0], &iflag));
+        int its = 0, nref = 0;
+        iflag = 0;
+        phist_b200_mixed_carp_solve(M, Bj, Xj, om.data(), tol, innerTol, maxIter, maxRefine, &its, &nref, &iflag);
+        if (iflag < 0) {
+          fprintf(stderr, "mixed_carp_solve returned %d\n", iflag);
+          return 1;
+        }
+        iters.push_back(its);
+        refines.push_back(nref);
+        CHK(phist_b200_mixed_carp_delete(M, &iflag));
+      } else {
+        phist_Dcarp_cgState_ptr S = NULL;
+        CHK(phist_Dcarp_cgState_create(&S, A, NULL, w, &shifts[j0], NULL, &iflag));
+        for (int j = 0; j < w; j++) S->omega_[j] = omega;
+        CHK(phist_Dcarp_cgState_reset(S, Bj, NULL, &iflag));
+        iflag = 0;
+        phist_Dcarp_cgState_iterate(S, Xj, NULL, tol, maxIter, 0, &iflag);
+        if (iflag < 0) {
+          fprintf(stderr, "carp_cgState_iterate returned %d\n", iflag);
+          return 1;
+        }
+        iters.push_back(S->numIter);
+        for (int j = 0; j < w; j++) conv[j0 + j] = S->conv[j];
+        CHK(phist_Dcarp_cgState_delete(S, &iflag));
       }
-      iters.push_back(S->numIter);
-      for (int j = 0; j < w; j++) conv[j0 + j] = S->conv[j];
-      CHK(phist_Dcarp_cgState_delete(S, &iflag));
       CHK(phist_Dmvec_delete(Xj, &iflag));
       CHK(phist_Dmvec_delete(Bj, &iflag));
     }
@@ -163,6 +189,9 @@ int main(int argc, char** argv)
     CHK(phist_Dmvec_norm2(B, nb.data(), &iflag));
     CHK(phist_Dmvec_norm2(R, nr.data(), &iflag));
     for (int j = 0; j < nshifts; j++) relres[j] = nr[j] / nb[j];
+    // the refinement loop stops on exactly this FP64 residual test
+    if (mixed)
+      for (int j = 0; j < nshifts; j++) conv[j] = nr[j] <= tol * nb[j];
   }
   int nconv = 0;
   double maxres = 0.0;
@@ -170,9 +199,12 @@ int main(int argc, char** argv)
     nconv += conv[j];
     maxres = std::max(maxres, relres[j]);
   }
-  printf("{\"problem\": \"%s\", \"n\": %d, \"nshifts\": %d, \"block\": %d, \"tol\": %.3e, \"maxIter\": %d, "
+  printf("{\"problem\": \"%s\", \"mixed\": %d, \"innerTol\": %.3e, \"refinements\": [", problem, mixed,
+         innerTol);
+  for (size_t i = 0; i < refines.size(); i++) printf("%s%d", i ? ", " : "", refines[i]);
+  printf("], \"n\": %d, \"nshifts\": %d, \"block\": %d, \"tol\": %.3e, \"maxIter\": %d, "
          "\"omega\": %g, \"nconv\": %d, \"max_relres\": %.6e, \"launches\": %llu, \"iters\": [",
-         problem, nloc, nshifts, block, tol, maxIter, omega, nconv, maxres, (unsigned long long)launches);
+         nloc, nshifts, block, tol, maxIter, omega, nconv, maxres, (unsigned long long)launches);
   for (size_t i = 0; i < iters.size(); i++) printf("%s%d", i ? ", " : "", iters[i]);
   printf("], \"wall\": [");
   for (size_t i = 0; i < walls.size(); i++) printf("%s%.6f", i ? ", " : "", walls[i]);

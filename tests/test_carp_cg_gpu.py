@@ -68,3 +68,23 @@ def test_carp_cg_honeycomb_shifts(session, tmp_path, nshifts, block):
         cond = np.abs(lam - shifts[j]).max() / np.abs(lam - shifts[j]).min()
         err = np.linalg.norm(x[:, j] - xs) / np.linalg.norm(xs)
         assert err <= cond * 4 * tol, (j, err, cond)
+
+
+def test_carp_cg_mixed_refinement(session, tmp_path):
+    """FP32 CARP-CG sweeps inside FP64 iterative refinement reach the same
+    FP64 relative residual as the all-FP64 solver"""
+    from phist_b200.generators import honeycomb, unif
+    L, seed, tol, ns = 24, 4, 1e-10, 8
+    out = str(tmp_path / "x.bin")
+    r = run("HONEYCOMB-%d-S%d-W1" % (L, seed), "nshifts=%d" % ns, "block=4", "tol=%g" % tol,
+            "maxIter=40000", "seed=%d" % seed, "mixed=1", "innerTol=1e-5", "out=" + out)
+    assert r["mixed"] == 1 and r["nconv"] == ns
+    assert all(k >= 2 for k in r["refinements"])
+    rp, c, v = honeycomb(L, L, seed)
+    n = len(rp) - 1
+    shifts = 2.5 * unif(seed, np.arange(ns, dtype=np.uint64))
+    b = np.stack([unif(seed + 1 + j, np.arange(n, dtype=np.uint64)) for j in range(ns)], 1)
+    x = np.fromfile(out, dtype=np.float64).reshape(n, ns)
+    res = b - (crs_matvec(rp, c, v, x) - shifts[None, :] * x)
+    rel = np.linalg.norm(res, axis=0) / np.linalg.norm(b, axis=0)
+    assert rel.max() <= 2 * tol, rel
