@@ -161,7 +161,9 @@ int main(int argc, char** argv)
         CHK(phist_b200_mixed_carp_delete(M, &iflag));
       } else {
         phist_Dcarp_cgState_ptr S = NULL;
-        CHK(phist_Dcarp_cgState_create(&S, A, NULL, w, &shifts[j0], NULL, &iflag));
+        // carp_cgState_create reads sigma_i[j] for every j (phist_carp_cg_def.hpp:131-135)
+        std::vector<double> zeros(w, 0.0);
+        CHK(phist_Dcarp_cgState_create(&S, A, NULL, w, &shifts[j0], zeros.data(), &iflag));
         for (int j = 0; j < w; j++) S->omega_[j] = omega;
         CHK(phist_Dcarp_cgState_reset(S, Bj, NULL, &iflag));
         iflag = 0;

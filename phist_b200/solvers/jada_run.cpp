@@ -12,6 +12,7 @@
 //   jada_run <problem> [key=value ...]
 //   keys: numEigs which(SR|LR|SM|LM|TARGET) blockSize minBas maxBas convTol
 //         maxIters innerSolvType(GMRES|MINRES) innerSolvMaxIters symmetry(GENERAL|HERMITIAN)
+//         target arno initialShiftIters (fixed shift for the first iterations)
 //         seed (start block uniform[-1,1) from this seed) sigma (SELL sigma)
 //         reps (repeat the solve, report each wall time)
 //         mixed=1 (FP32 correction equations through pb_mixed_jada.h; the
@@ -106,6 +107,8 @@ int main(int argc, char** argv)
     else if (k == "innerSolvMaxIters") opts.innerSolvMaxIters = atoi(v);
     else if (k == "symmetry") opts.symmetry = str2matSym(v);
     else if (k == "target") { opts.initialShift_r = atof(v); }
+    else if (k == "arno") opts.arno = atoi(v);
+    else if (k == "initialShiftIters") opts.initialShiftIters = atoi(v);
     else if (k == "seed") seed = strtoull(v, nullptr, 10);
     else if (k == "sigma") sigma = atoll(v);
     else if (k == "reps") reps = atoi(v);

@@ -21,7 +21,7 @@ struct pb_mixed_carp {
   phist_SsparseMat_ptr As = nullptr;
   int nsys = 0;
   std::vector<double> sigma, negSigma;
-  std::vector<float> sigmaS;
+  std::vector<float> sigmaS, zerosS;
   phist_Scarp_cgState_ptr S = nullptr;
   phist_Dmvec_ptr R = nullptr, D = nullptr;
   phist_Smvec_ptr Rs = nullptr, Ds = nullptr;
@@ -64,6 +64,7 @@ extern "C" void phist_b200_mixed_carp_create(pb_mixed_carp** out, void const* A,
   me->sigma.assign(sigma, sigma + nsys);
   me->negSigma.resize(nsys);
   me->sigmaS.resize(nsys);
+  me->zerosS.assign(nsys, 0.0f);  // carp_cgState_create reads sigma_i[j] for every j
   for (int j = 0; j < nsys; j++) {
     me->negSigma[j] = -sigma[j];
     me->sigmaS[j] = (float)sigma[j];
@@ -76,7 +77,7 @@ extern "C" void phist_b200_mixed_carp_create(pb_mixed_carp** out, void const* A,
   if (*iflag == 0) phist_Dmvec_create(&me->D, mapD, nsys, iflag);
   if (*iflag == 0) phist_Smvec_create(&me->Rs, mapS, nsys, iflag);
   if (*iflag == 0) phist_Smvec_create(&me->Ds, mapS, nsys, iflag);
-  if (*iflag == 0) phist_Scarp_cgState_create(&me->S, me->As, nullptr, nsys, me->sigmaS.data(), nullptr, iflag);
+  if (*iflag == 0) phist_Scarp_cgState_create(&me->S, me->As, nullptr, nsys, me->sigmaS.data(), me->zerosS.data(), iflag);
   if (*iflag != 0) {
     const int e = *iflag;
     release(me);

@@ -13,6 +13,7 @@
 #include <cstdio>
 #include <cstring>
 #include <new>
+#include <vector>
 
 #include "phist_config.h"
 #include "phist_kernels.h"
@@ -102,6 +103,20 @@ static void pb_mixed_jada_run(void* data, void const* A_op, void const* B_op, vo
   PB_CHK(me->T.view(me->map, k, iflag));
   PB_CHK(phist_b200_mvec_DtoS((phist_Dconst_mvec_ptr)Qtil, me->Q.v, iflag));
   PB_CHK(phist_b200_mvec_DtoS((phist_Dconst_mvec_ptr)res, me->R.v, iflag));
+  // Scale every right-hand side to norm 1024.  PHIST's blocked GMRES counts a
+  // system as converged once its residual is below 1000 eps of the type in
+  // absolute terms (phist_blockedgmres_def.hpp:606,970), i.e. 1.2e-4 in FP32:
+  // late Jacobi-Davidson residuals are smaller than that and would return
+  // t = 0.  The correction equation is linear in r and the solver returns
+  // t normalised (phist_jadaCorrectionSolver_def.hpp:583, end of the GMRES
+  // branch), so the scaling changes nothing else.
+  {
+    std::vector<double> nr(nres);
+    std::vector<float> sc(nres);
+    PB_CHK(phist_Dmvec_norm2((phist_Dconst_mvec_ptr)res, nr.data(), iflag));
+    for (int j = 0; j < nres; j++) sc[j] = nr[j] > 0.0 ? (float)(1024.0 / nr[j]) : 1.0f;
+    PB_CHK(phist_Smvec_vscale(me->R.v, sc.data(), iflag));
+  }
 
   float s[64], tl[64];
   if (k > 64) {
