@@ -3,6 +3,7 @@
 // phist_kernels_fused_decl.h, phist_kernels_carp_decl.h).  Instantiated for
 // double (phist_D*) in pb_api_D.cu and float (phist_S*) in pb_api_S.cu.
 #pragma once
+#include <cudaTypedefs.h>
 #include <algorithm>
 #include <cmath>
 #include <numeric>
@@ -24,7 +25,6 @@ inline bool vec_ok(const T* p, int64_t ld, int ncols)
   const int vw = 16 / (int)sizeof(T);
   return (((uintptr_t)p) & 15u) == 0 && ld % vw == 0 && ncols % vw == 0;
 }
-inline int pad_width(int w) { return w <= 16 ? 16 : w <= 32 ? 32 : 64; }
 
 // raise a kernel's dynamic shared-memory limit once (the attribute call is a
 // host round trip that would otherwise precede every launch)
@@ -294,10 +294,22 @@ void sd_upload(SdMat<T>* M)
   PB_CUDA(cudaMemcpy2DAsync(M->d(), M->lda * sizeof(T), M->h(), M->lda * sizeof(T),
                             M->nrows * sizeof(T), M->ncols, cudaMemcpyHostToDevice, stream()));
 }
+// Device -> host copy of an sdMat.  Small matrices (all the solvers' Gram and
+// projection matrices) go through the pinned mailbox: one asynchronous DMA,
+// one stream synchronisation and a host copy, instead of a pageable transfer.
 template <class T>
 void sd_download(SdMat<T>* M)
 {
   if (M->nrows == 0 || M->ncols == 0) return;
+  const size_t col = sizeof(T) * (size_t)M->nrows;
+  if (col * (size_t)M->ncols <= Runtime::kMailboxResultBytes) {
+    char* hb = (char*)rt().mailbox_host();
+    PB_CUDA(cudaMemcpy2DAsync(hb, col, M->d(), M->lda * sizeof(T), col, M->ncols, cudaMemcpyDeviceToHost,
+                              stream()));
+    rt().sync();
+    for (int j = 0; j < M->ncols; j++) memcpy(M->h() + (int64_t)j * M->lda, hb + col * j, col);
+    return;
+  }
   PB_CUDA(cudaMemcpy2DAsync(M->h(), M->lda * sizeof(T), M->d(), M->lda * sizeof(T),
                             M->nrows * sizeof(T), M->ncols, cudaMemcpyDeviceToHost, stream()));
   rt().sync();
@@ -739,7 +751,9 @@ void spmv_general(T alpha, const SparseMat<T>* A, const T* shifts, const Mvec<T>
       k_axpby<T><<<grid_for((int64_t)Y->nrows * nvec), 256, 0, stream()>>>(Y->d(), Y->lda, U->d(), U->lda, Y->nrows, nvec, gamma, nullptr, delta);
       PB_LAUNCH_CHECK();
     }
-    T* dd = (T*)rt().dmalloc(sizeof(T) * 64);
+    // dots written by the final reduction straight into the mapped mailbox
+    T* dd = (T*)rt().mailbox_dev();
+    const T* hbox = (const T*)rt().mailbox_host();
     for (int c0 = 0; c0 < nvec; c0 += 64) {
       const int nv = std::min(64, nvec - c0);
       auto dotk = [&](const Mvec<T>* P, int poff, T* out) {
@@ -747,23 +761,17 @@ void spmv_general(T alpha, const SparseMat<T>* A, const T* shifts, const Mvec<T>
         T* part = (T*)rt().scratch(sizeof(T) * (size_t)grid * 64);
         k_coldot<T, 64><<<grid, 256, 0, stream()>>>(P->d() + poff, P->lda, Y->d() + c0, Y->lda, Y->nrows, nv, part, rt().counters(), dd);
         PB_LAUNCH_CHECK();
-        std::vector<T> h(64);
-        PB_CUDA(cudaMemcpyAsync(h.data(), dd, sizeof(T) * 64, cudaMemcpyDeviceToHost, stream()));
         rt().sync();
-        for (int j = 0; j < nv; j++) out[c0 + j] = h[j];
+        for (int j = 0; j < nv; j++) out[c0 + j] = hbox[j];
       };
       if (WdotW) dotk(Y, c0, WdotW);
       if (VdotW) dotk(X, c0, VdotW);
     }
-    rt().dfree(dd);
     return;
   }
-  T* dots_dev = nullptr;
-  std::vector<T> hd;
-  if (WdotW || VdotW) {
-    dots_dev = (T*)rt().dmalloc(sizeof(T) * 64);
-    hd.resize(64);
-  }
+  // fused dots: the kernel's final reduction writes into the mapped mailbox
+  T* dots_dev = (WdotW || VdotW) ? (T*)rt().mailbox_dev() : nullptr;
+  const T* hd = (const T*)rt().mailbox_host();
   for (int c0 = 0; c0 < nvec; c0 += 32) {
     const int nv = std::min(32, nvec - c0);
     SpmvArgs<T> p;
@@ -789,7 +797,6 @@ void spmv_general(T alpha, const SparseMat<T>* A, const T* shifts, const Mvec<T>
     spmv_tile<T>(A, p, nv);
     if (dots_dev) {
       const int NV = nv <= 1 ? 1 : nv <= 2 ? 2 : nv <= 4 ? 4 : nv <= 8 ? 8 : nv <= 16 ? 16 : 32;
-      PB_CUDA(cudaMemcpyAsync(hd.data(), dots_dev, sizeof(T) * 2 * NV, cudaMemcpyDeviceToHost, stream()));
       rt().sync();
       for (int j = 0; j < nv; j++) {
         if (WdotW) WdotW[c0 + j] = hd[j];
@@ -797,12 +804,133 @@ void spmv_general(T alpha, const SparseMat<T>* A, const T* shifts, const Mvec<T>
       }
     }
   }
-  if (dots_dev) rt().dfree(dots_dev);
 }
 
 // ======================================================================
 // block products
 // ======================================================================
+// cuTensorMapEncodeTiled through the runtime's driver entry point (no
+// link-time dependency on libcuda)
+inline PFN_cuTensorMapEncodeTiled_v12000 tmap_encoder()
+{
+  static PFN_cuTensorMapEncodeTiled_v12000 fn = nullptr;
+  static std::once_flag once;
+  std::call_once(once, [] {
+    void* p = nullptr;
+    cudaDriverEntryPointQueryResult q;
+    if (cudaGetDriverEntryPoint("cuTensorMapEncodeTiled", &p, cudaEnableDefault, &q) == cudaSuccess &&
+        q == cudaDriverEntryPointSuccess)
+      fn = (PFN_cuTensorMapEncodeTiled_v12000)p;
+    else
+      cudaGetLastError();
+  });
+  return fn;
+}
+
+// 2D tensor map of a row-major block (nrows x ncols, leading dimension ld)
+// with boxes of box_rows x box_cols (columns past ncols read as zero).
+// False where TMA cannot describe the block: base not 16-byte aligned, row
+// stride not a multiple of 16 bytes, or a box beyond the hardware limits.
+template <class T>
+bool make_rows_tmap(CUtensorMap* map, const T* base, int64_t nrows, int ncols, int64_t ld, int box_cols,
+                    int box_rows)
+{
+  auto fn = tmap_encoder();
+  if (!fn || nrows < 1 || ncols < 1 || nrows >= (int64_t(1) << 31)) return false;
+  if ((((uintptr_t)base) & 15u) != 0 || ((size_t)ld * sizeof(T)) % 16 != 0) return false;
+  if (box_cols > 256 || box_rows > 256 || ((size_t)box_cols * sizeof(T)) % 16 != 0) return false;
+  cuuint64_t dims[2] = {(cuuint64_t)ncols, (cuuint64_t)nrows};
+  cuuint64_t strides[1] = {(cuuint64_t)((size_t)ld * sizeof(T))};
+  cuuint32_t box[2] = {(cuuint32_t)box_cols, (cuuint32_t)box_rows};
+  cuuint32_t estr[2] = {1, 1};
+  const CUresult r = fn(map, sizeof(T) == 8 ? CU_TENSOR_MAP_DATA_TYPE_FLOAT64 : CU_TENSOR_MAP_DATA_TYPE_FLOAT32, 2,
+                        (void*)base, dims, strides, box, estr, CU_TENSOR_MAP_INTERLEAVE_NONE,
+                        CU_TENSOR_MAP_SWIZZLE_NONE, CU_TENSOR_MAP_L2_PROMOTION_L2_256B,
+                        CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE);
+  return r == CUDA_SUCCESS;
+}
+
+inline int pad_width5(int w) { return w <= 4 ? 4 : w <= 8 ? 8 : w <= 16 ? 16 : w <= 32 ? 32 : 64; }
+
+// k_mvtmv_async launch for padded widths BM x BK: micro-tile TT by output
+// size; R rows per stage sized for about 32 KiB of staged rows, 3 stages,
+// two blocks per SM (the reduction buffer may need more shared memory for
+// the widest tiles, which are compute-bound anyway)
+template <class T, int BM, int BK>
+void mvtmv_async_launch(MvTmvArgs<T>& a, int64_t n)
+{
+  constexpr int TT = (BM * BK <= 64) ? 2 : (BM * BK <= 1024) ? 4 : 8;
+  constexpr int VWd = 16 / (int)sizeof(T);
+  constexpr int PV = BM + VWd, PW = BK + VWd;
+  constexpr int RR = ((32768 / (int)sizeof(T)) / (PV + PW)) / 16 * 16;
+  constexpr int R = RR < 16 ? 16 : RR;
+  constexpr int S = 3;
+  constexpr int NT = (BM / TT) * (BK / TT), RG = 256 / NT;
+  const size_t stage = sizeof(T) * (size_t)S * R * (PV + PW);
+  const size_t red = sizeof(T) * (size_t)RG * BM * BK;
+  const size_t smem = std::max(stage, red);
+  const int grid = (int)std::min<int64_t>(ceil_div(n > 0 ? n : 1, R), (int64_t)rt().num_sms() * 2);
+  a.part = (T*)rt().scratch(sizeof(T) * (size_t)grid * a.m * a.k);
+  a.counter = rt().counters();
+  a.R = R;
+  // many outputs: the cross-block sum as a second, GPU-wide pass
+  const int nout = a.m * a.k;
+  a.ext_reduce = (nout >= 64 && grid > 1) ? 1 : 0;
+  // TMA staging where both blocks can be described by tensor maps
+  constexpr int RT = R > 256 ? 256 : R;
+  CUtensorMap mapV, mapW;
+  if (rt().use_tma && make_rows_tmap<T>(&mapV, a.V, n, a.m, a.ldv, PV, RT) &&
+      make_rows_tmap<T>(&mapW, a.W, n, a.k, a.ldw, PW, RT)) {
+    const size_t tstage = sizeof(T) * (size_t)S * RT * (PV + PW) + 8 * S;
+    const size_t tsmem = std::max(tstage, red);
+    const int tgrid = (int)std::min<int64_t>(ceil_div(n, RT), (int64_t)rt().num_sms() * 2);
+    a.part = (T*)rt().scratch(sizeof(T) * (size_t)tgrid * a.m * a.k);
+    a.ext_reduce = (nout >= 64 && tgrid > 1) ? 1 : 0;
+    a.R = RT;
+    auto kern = k_mvtmv_tma<T, BM, BK, TT, RT, S>;
+    set_smem(kern, tsmem);
+    kern<<<tgrid, BLK_BS, tsmem, stream()>>>(a, mapV, mapW, rt().device_error_word());
+    if (a.ext_reduce) {
+      PB_LAUNCH_CHECK();
+      k_reduce_partials<T><<<(nout + 31) / 32, 256, 0, stream()>>>(a.part, tgrid, nout, a.Cd, a.m, a.ldc, a.alpha,
+                                                                    a.beta);
+    }
+    return;
+  }
+  auto kern = k_mvtmv_async<T, BM, BK, TT, R, S>;
+  set_smem(kern, smem);
+  kern<<<grid, BLK_BS, smem, stream()>>>(a);
+  if (a.ext_reduce) {
+    PB_LAUNCH_CHECK();
+    k_reduce_partials<T><<<(nout + 31) / 32, 256, 0, stream()>>>(a.part, grid, nout, a.Cd, a.m, a.ldc, a.alpha,
+                                                                  a.beta);
+  }
+}
+
+template <class T, int BM>
+void mvtmv_async_bk(MvTmvArgs<T>& a, int64_t n, int BK)
+{
+  switch (BK) {
+    case 4: mvtmv_async_launch<T, BM, 4>(a, n); break;
+    case 8: mvtmv_async_launch<T, BM, 8>(a, n); break;
+    case 16: mvtmv_async_launch<T, BM, 16>(a, n); break;
+    case 32: mvtmv_async_launch<T, BM, 32>(a, n); break;
+    default: mvtmv_async_launch<T, BM, 64>(a, n); break;
+  }
+}
+
+template <class T>
+void mvtmv_async(MvTmvArgs<T>& a, int64_t n, int BM, int BK)
+{
+  switch (BM) {
+    case 4: mvtmv_async_bk<T, 4>(a, n, BK); break;
+    case 8: mvtmv_async_bk<T, 8>(a, n, BK); break;
+    case 16: mvtmv_async_bk<T, 16>(a, n, BK); break;
+    case 32: mvtmv_async_bk<T, 32>(a, n, BK); break;
+    default: mvtmv_async_bk<T, 64>(a, n, BK); break;
+  }
+}
+
 template <class T>
 void launch_mvTmv(int64_t n, int m, int k, T alpha, const T* V, int64_t ldv, const T* W,
                   int64_t ldw, T beta, T* Cd, int64_t ldc)
@@ -810,8 +938,14 @@ void launch_mvTmv(int64_t n, int m, int k, T alpha, const T* V, int64_t ldv, con
   MvTmvArgs<T> a;
   a.n = n; a.m = m; a.k = k; a.V = V; a.ldv = ldv; a.W = W; a.ldw = ldw;
   a.alpha = alpha; a.beta = beta; a.Cd = Cd; a.ldc = ldc;
+  if (m <= 64 && k <= 64 && vec_ok(V, ldv, m) && vec_ok(W, ldw, k)) {
+    // multi-stage asynchronously staged row tiles, widths padded to 4..64
+    mvtmv_async<T>(a, n, pad_width5(m), pad_width5(k));
+    PB_LAUNCH_CHECK();
+    return;
+  }
   if (m <= 8 && k <= 8) {
-    // register kernel: padded widths M (4|8) and K (1|4|8)
+    // register kernel (odd or unaligned widths): padded widths M (4|8) and K (1|4|8)
     const int M = m <= 4 ? 4 : 8, K = k == 1 ? 1 : k <= 4 ? 4 : 8;
     const int grid = std::max(1, std::min(grid_for(n), rt().num_sms() * 4));
     a.part = (T*)rt().scratch(sizeof(T) * (size_t)grid * M * K);
@@ -824,36 +958,6 @@ void launch_mvTmv(int64_t n, int m, int k, T alpha, const T* V, int64_t ldv, con
       if (K == 1) PB_MVR(8, 1); else if (K == 4) PB_MVR(8, 4); else PB_MVR(8, 8);
     }
 #undef PB_MVR
-    PB_LAUNCH_CHECK();
-    return;
-  }
-  if (m <= 64 && k <= 64 && vec_ok(V, ldv, m) && vec_ok(W, ldw, k)) {
-    // asynchronously staged tiles, widths padded to 16/32/64
-    const int BM = pad_width(m), BK = pad_width(k);
-    const int TT = (BM * BK >= 2048) ? 8 : 4;
-    constexpr int R = 64;
-    const int NT = (BM / TT) * (BK / TT), RG = BLK_BS / NT;
-    const size_t stage = sizeof(T) * 2 * R * (size_t)(BM + BK);
-    const size_t red = sizeof(T) * (size_t)RG * BM * BK;
-    const size_t smem = std::max(stage, red);
-    const int grid = (int)std::min<int64_t>(ceil_div(n > 0 ? n : 1, R), (int64_t)rt().num_sms() * (TT == 8 ? 1 : 2));
-    a.part = (T*)rt().scratch(sizeof(T) * (size_t)grid * m * k);
-    a.counter = rt().counters();
-    a.R = R;
-#define PB_MVA(BMv, BKv, TTv)                                                                  \
-  {                                                                                            \
-    auto kern = k_mvtmv_async<T, BMv, BKv, TTv, R>;                                            \
-    set_smem(kern, smem); \
-    kern<<<grid, BLK_BS, smem, stream()>>>(a);                                                 \
-  }
-    if (BM == 16) {
-      if (BK == 16) PB_MVA(16, 16, 4) else if (BK == 32) PB_MVA(16, 32, 4) else PB_MVA(16, 64, 4)
-    } else if (BM == 32) {
-      if (BK == 16) PB_MVA(32, 16, 4) else if (BK == 32) PB_MVA(32, 32, 4) else PB_MVA(32, 64, 8)
-    } else {
-      if (BK == 16) PB_MVA(64, 16, 4) else if (BK == 32) PB_MVA(64, 32, 8) else PB_MVA(64, 64, 8)
-    }
-#undef PB_MVA
     PB_LAUNCH_CHECK();
     return;
   }
@@ -884,9 +988,64 @@ void launch_mvTmv(int64_t n, int m, int k, T alpha, const T* V, int64_t ldv, con
   PB_LAUNCH_CHECK();
 }
 
+// k_mvsd_async launch for padded widths BM x BK: TC output columns per
+// thread (TX = BK/TC threads per row), TR rows per thread, sized for about
+// 24 KiB of staged input rows per stage; 4 stages (3 where a stage is
+// larger), two blocks per SM
+template <class T, int BM, int BK>
+void mvsd_async_launch(RowGemmArgs<T>& a)
+{
+  constexpr int TC = BK >= 16 ? 4 : BK / 4;
+  constexpr int TX = BK / TC, TY = 256 / TX;
+  constexpr int AP = BM + 16 / (int)sizeof(T);
+  constexpr int TR0 = 24576 / (TY * AP * (int)sizeof(T));
+  constexpr int TR = TR0 < 1 ? 1 : TR0 > 8 ? 8 : TR0;
+  constexpr int R = TY * TR;
+  constexpr int S = (R * AP * (int)sizeof(T) > 30000) ? 3 : 4;
+  const size_t smem = sizeof(T) * ((size_t)BM * BK + (size_t)S * R * AP);
+  const int grid = (int)std::min<int64_t>(ceil_div(a.n > 0 ? a.n : 1, R), (int64_t)rt().num_sms() * 2);
+  auto kern = k_mvsd_async<T, BM, BK, TR, TC, S>;
+  set_smem(kern, smem);
+  kern<<<grid, BLK_BS, smem, stream()>>>(a);
+}
+
+template <class T, int BM>
+void mvsd_async_bk(RowGemmArgs<T>& a, int BK)
+{
+  switch (BK) {
+    case 4: mvsd_async_launch<T, BM, 4>(a); break;
+    case 8: mvsd_async_launch<T, BM, 8>(a); break;
+    case 16: mvsd_async_launch<T, BM, 16>(a); break;
+    case 32: mvsd_async_launch<T, BM, 32>(a); break;
+    default: mvsd_async_launch<T, BM, 64>(a); break;
+  }
+}
+
+template <class T>
+void mvsd_async(RowGemmArgs<T>& a, int BM, int BK)
+{
+  switch (BM) {
+    case 4: mvsd_async_bk<T, 4>(a, BK); break;
+    case 8: mvsd_async_bk<T, 8>(a, BK); break;
+    case 16: mvsd_async_bk<T, 16>(a, BK); break;
+    case 32: mvsd_async_bk<T, 32>(a, BK); break;
+    default: mvsd_async_bk<T, 64>(a, BK); break;
+  }
+}
+
 template <class T>
 void launch_rowgemm(RowGemmArgs<T>& a)
 {
+  {
+    // gram-free V*C and in-place W*C on aligned widths: multi-stage staged tiles
+    const T* A = (a.mode == RM_MVSDI) ? (const T*)a.W : a.V;
+    const int64_t lda = (a.mode == RM_MVSDI) ? a.ldw : a.ldv;
+    if (a.gram == GM_NONE && a.mode != RM_VCWD && a.m <= 64 && a.k <= 64 && vec_ok(A, lda, a.m)) {
+      mvsd_async<T>(a, pad_width5(a.m), pad_width5(a.k));
+      PB_LAUNCH_CHECK();
+      return;
+    }
+  }
   if (a.m <= 8 && a.k <= 8 && (a.gram != GM_VW || a.mv <= 8)) {
     // register kernel: padded widths M (4|8), K (1|4|8), MV (1, or 8 for V'W)
     const int M = a.m <= 4 ? 4 : 8, K = a.k == 1 ? 1 : a.k <= 4 ? 4 : 8;
@@ -916,21 +1075,8 @@ void launch_rowgemm(RowGemmArgs<T>& a)
     const bool gram_ok = a.gram == GM_NONE || (vec_ok((const T*)a.W, a.ldw, a.k) &&
                                                (a.gram == GM_WW || (a.mv <= 64 && vec_ok(a.Vg, a.ldvg, a.mv))));
     if (gram_ok && a.mode != RM_VCWD && a.m <= 64 && a.k <= 64 && vec_ok(A, lda, a.m)) {
-      // asynchronously staged row tiles of 64 rows, widths padded to 16/32/64
-      const int BM = pad_width(a.m), BK = pad_width(a.k);
-      const size_t smem = sizeof(T) * ((size_t)BM * BK + 2 * 64 * (size_t)(BM + 16 / sizeof(T)));
-      const int grid = (int)std::min<int64_t>(ceil_div(a.n > 0 ? a.n : 1, 64), (int64_t)rt().num_sms() * 2);
-#define PB_MSA(BMv, BKv, TRv)                                                                  \
-  {                                                                                            \
-    auto kern = k_mvsd_async<T, BMv, BKv, TRv, 4>;                                             \
-    set_smem(kern, smem); \
-    kern<<<grid, BLK_BS, smem, stream()>>>(a);                                                 \
-  }
-#define PB_MSA_K(BMv)                                                  \
-  if (BK == 16) PB_MSA(BMv, 16, 1) else if (BK == 32) PB_MSA(BMv, 32, 2) else PB_MSA(BMv, 64, 4)
-      if (BM == 16) { PB_MSA_K(16) } else if (BM == 32) { PB_MSA_K(32) } else { PB_MSA_K(64) }
-#undef PB_MSA_K
-#undef PB_MSA
+      // multi-stage staged row tiles, widths padded to 4..64
+      mvsd_async<T>(a, pad_width5(a.m), pad_width5(a.k));
       PB_LAUNCH_CHECK();
       // fused Gram at these widths: a second pass over the new W with the
       // staged Gram kernel (the register kernels above fuse it into one pass)

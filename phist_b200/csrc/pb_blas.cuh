@@ -106,7 +106,7 @@ __global__ void k_copy(const TI* __restrict__ x, int64_t ldx, TO* y, int64_t ldy
 template <class T, int NV>
 __global__ void __launch_bounds__(256)
 k_coldot(const T* __restrict__ v, int64_t ldv, const T* __restrict__ w, int64_t ldw, int64_t n,
-         int nvec, T* part, unsigned int* counter, T* out)
+         int nvec, T* part, unsigned int* counter, T* out, int ext = 0)
 {
   T acc[NV];
 #pragma unroll
@@ -132,6 +132,7 @@ k_coldot(const T* __restrict__ v, int64_t ldv, const T* __restrict__ w, int64_t 
     for (int w2 = 0; w2 < (int)(blockDim.x >> 5); w2++) s += red[w2][threadIdx.x];
     part[(int64_t)blockIdx.x * NV + threadIdx.x] = s;
   }
+  if (ext) return;  // second pass: k_reduce_partials
   last_block_reduce<T>(part, NV, gridDim.x, counter, out, 1, NV, 0, T(1), T(0));
 }
 

@@ -72,6 +72,7 @@ struct MvTmvArgs {
   T* Cd; int64_t ldc;          // device result (col-major)
   T* part; unsigned int* counter;
   int R;                        // rows per tile
+  int ext_reduce;               // k_mvtmv_async: leave the partials to k_reduce_partials
 };
 
 // thread (tm, tk, g): output micro-tile rows [tm*TM, +TM) of V' and columns

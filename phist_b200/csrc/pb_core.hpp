@@ -133,6 +133,20 @@ class Runtime {
   void* scratch(size_t bytes);
   unsigned int* counters();  // 64 zero-initialised counters
 
+  // Result mailbox: kMailboxBytes of pinned host memory mapped into the
+  // device address space.  Calls that return values to the host (dots,
+  // norms, Gram matrices) have their final kernel or copy write here and
+  // read it after one stream synchronisation, with no pageable staging copy.
+  // One stream and one host thread use it, one call at a time.
+  static constexpr size_t kMailboxBytes = 1u << 20;
+  // results use the first kMailboxResultBytes; the last 64 bytes hold the
+  // device error word (kernels with bounded waits store a code there, and
+  // sync() reports and clears it)
+  static constexpr size_t kMailboxResultBytes = kMailboxBytes - 64;
+  void* mailbox_host() { if (!inited_) init(); return mbox_h_; }
+  void* mailbox_dev() { if (!inited_) init(); return mbox_d_; }
+  int* device_error_word() { if (!inited_) init(); return (int*)((char*)mbox_d_ + kMailboxResultBytes); }
+
   // SELL parameters used for new matrices (C chunk height, sigma window)
   int sell_C = 32;
   int64_t sell_sigma_default = 256;  // when PERM_LOCAL is requested
@@ -147,6 +161,8 @@ class Runtime {
   // than the register kernel on the 3D Anderson matrix (nvec 8/16/32:
   // 219/436/1077 us against 152/285/545 us).
   int spmv_staged_min_nvec = 99;
+  // stage block-vector tiles of the Gram kernels with TMA (else cp.async)
+  bool use_tma = true;
 
   // statistics: kernel launches issued by this library
   uint64_t launches = 0;
@@ -163,6 +179,8 @@ class Runtime {
   void* scratch_ = nullptr;
   size_t scratch_bytes_ = 0;
   unsigned int* counters_ = nullptr;
+  void* mbox_h_ = nullptr;
+  void* mbox_d_ = nullptr;
 };
 
 inline Runtime& rt() { return Runtime::get(); }

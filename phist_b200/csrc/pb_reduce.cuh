@@ -92,3 +92,49 @@ __device__ __forceinline__ bool last_block_reduce(const T* part, int nout, int n
 }
 
 }  // namespace pb
+
+namespace pb {
+
+// Second pass of a two-level reduction for many outputs.  The last-block
+// reduction above runs on one SM; with nout*nblocks partials in the tens of
+// thousands that SM's serial chains of L2 loads dominate the call.  Here a
+// block owns 32 consecutive outputs (lanes: coalesced rows of the partials)
+// and splits the partial blocks into 8 fixed chunks (warps); chunk sums are
+// combined in chunk order, so the result is independent of timing.
+//   out(i, j) = alpha * sum_b part[b*nout + o] + beta * out(i, j),
+//   o = i + j*mrows, out(i, j) at C[i + j*ldc]
+template <class T>
+__global__ void __launch_bounds__(256) k_reduce_partials(const T* __restrict__ part, int nblocks, int nout,
+                                                         T* C, int mrows, int64_t ldc, T alpha, T beta)
+{
+  __shared__ T red[8][32];
+  const int ol = threadIdx.x & 31, ch = threadIdx.x >> 5;
+  const int o = blockIdx.x * 32 + ol;
+  T s = T(0);
+  if (o < nout) {
+    const int per = (nblocks + 7) / 8;
+    const int b0 = ch * per;
+    const int b1 = min(nblocks, b0 + per);
+    T s0 = T(0), s1 = T(0), s2 = T(0), s3 = T(0);
+    int b = b0;
+    for (; b + 4 <= b1; b += 4) {
+      s0 += __ldcg(part + (int64_t)b * nout + o);
+      s1 += __ldcg(part + (int64_t)(b + 1) * nout + o);
+      s2 += __ldcg(part + (int64_t)(b + 2) * nout + o);
+      s3 += __ldcg(part + (int64_t)(b + 3) * nout + o);
+    }
+    for (; b < b1; b++) s0 += __ldcg(part + (int64_t)b * nout + o);
+    s = (s0 + s1) + (s2 + s3);
+  }
+  red[ch][ol] = s;
+  __syncthreads();
+  if (ch == 0 && o < nout) {
+    T t = T(0);
+#pragma unroll
+    for (int c = 0; c < 8; c++) t += red[c][ol];
+    T* dst = C + (o % mrows) + (int64_t)(o / mrows) * ldc;
+    *dst = (beta == T(0)) ? alpha * t : alpha * t + beta * *dst;
+  }
+}
+
+}  // namespace pb

@@ -39,7 +39,12 @@ void Runtime::init()
   PB_CUDA(cudaStreamCreateWithFlags(&stream_, cudaStreamNonBlocking));
   PB_CUDA(cudaMalloc(&counters_, 64 * sizeof(unsigned int)));
   PB_CUDA(cudaMemset(counters_, 0, 64 * sizeof(unsigned int)));
+  // pinned, device-mapped result buffer for calls that return host data
+  PB_CUDA(cudaHostAlloc(&mbox_h_, kMailboxBytes, cudaHostAllocMapped));
+  PB_CUDA(cudaHostGetDevicePointer(&mbox_d_, mbox_h_, 0));
+  memset(mbox_h_, 0, kMailboxBytes);
   if (const char* v = getenv("PHIST_B200_VERBOSE")) verbose = atoi(v);
+  if (const char* v = getenv("PHIST_B200_TMA")) use_tma = atoi(v) != 0;
   if (const char* c = getenv("PHIST_B200_SELL_C")) sell_C = atoi(c);
   if (const char* s = getenv("PHIST_B200_SELL_SIGMA")) sell_sigma_default = atoll(s);
   inited_ = true;
@@ -59,6 +64,8 @@ void Runtime::finalize()
   scratch_bytes_ = 0;
   if (counters_) cudaFree(counters_);
   counters_ = nullptr;
+  if (mbox_h_) cudaFreeHost(mbox_h_);
+  mbox_h_ = mbox_d_ = nullptr;
   cudaStreamDestroy(stream_);
   stream_ = nullptr;
   inited_ = false;
@@ -123,7 +130,16 @@ void Runtime::hfree_pinned(void* p)
   if (p) cudaFreeHost(p);
 }
 
-void Runtime::sync() { PB_CUDA(cudaStreamSynchronize(stream_)); }
+void Runtime::sync()
+{
+  PB_CUDA(cudaStreamSynchronize(stream_));
+  volatile int* err = (volatile int*)((char*)mbox_h_ + kMailboxResultBytes);
+  if (mbox_h_ && *err != 0) {
+    const int e = *err;
+    *err = 0;
+    PB_THROW(PB_FUNCTIONAL_ERROR, "a device-side wait timed out (code %d); results of the last calls are invalid", e);
+  }
+}
 
 void* Runtime::scratch(size_t bytes)
 {

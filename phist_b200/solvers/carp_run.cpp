@@ -1,7 +1,8 @@
 // carp_run.cpp -- runs PHIST's unchanged CARP-CG solver
 // (phist_Dcarp_cgState_iterate, src/krylov/phist_carp_cg_def.hpp:304) for a
 // queue of real shifts on the b200 kernel library and prints one JSON line
-// with iteration counts, explicit relative residuals and wall times.
+// with explicit relative residuals (null where not finite), launch counts and
+// wall times.
 //
 // The call sequence follows PHIST's driver drivers/carp_cg.c:286-320: one
 // carp_cgState per block of shifts (create, reset with the right-hand sides,
@@ -61,6 +62,13 @@ static uint64_t mix64(uint64_t z)
   z = (z ^ (z >> 27)) * 0x94D049BB133111EBull;
   return z ^ (z >> 31);
 }
+// JSON number, null where not finite
+static void jnum(const char* sep, double v, const char* fmt)
+{
+  if (std::isfinite(v)) { printf("%s", sep); printf(fmt, v); }
+  else printf("%snull", sep);
+}
+
 static double unif(uint64_t seed, uint64_t idx)
 {
   const uint64_t h = mix64(seed * 0x632BE59BD9B4E019ull + mix64(idx));
@@ -130,11 +138,10 @@ int main(int argc, char** argv)
   }
 
   std::vector<double> walls, relres(nshifts, 0.0);
-  std::vector<int> iters, refines, conv(nshifts, 0);
+  std::vector<int> refines, conv(nshifts, 0);
   uint64_t launches = 0;
   for (int rep = 0; rep < reps; rep++) {
     CHK(phist_Dmvec_put_value(X, 0.0, &iflag));
-    iters.clear();
     refines.clear();
     uint64_t l0 = 0, l1 = 0;
     CHK(phist_b200_launch_count(&l0, &iflag));
@@ -149,14 +156,13 @@ int main(int argc, char** argv)
         pb_mixed_carp* M = NULL;
         std::vector<double> om(w, omega);
         CHK(phist_b200_mixed_carp_create(&M, A, w, &shifts[j0], &iflag));
-        int its = 0, nref = 0;
+        int nref = 0;
         iflag = 0;
-        phist_b200_mixed_carp_solve(M, Bj, Xj, om.data(), tol, innerTol, maxIter, maxRefine, &its, &nref, &iflag);
+        phist_b200_mixed_carp_solve(M, Bj, Xj, om.data(), tol, innerTol, maxIter, maxRefine, &nref, &iflag);
         if (iflag < 0) {
           fprintf(stderr, "mixed_carp_solve returned %d\n", iflag);
           return 1;
         }
-        iters.push_back(its);
         refines.push_back(nref);
         CHK(phist_b200_mixed_carp_delete(M, &iflag));
       } else {
@@ -172,7 +178,6 @@ int main(int argc, char** argv)
           fprintf(stderr, "carp_cgState_iterate returned %d\n", iflag);
           return 1;
         }
-        iters.push_back(S->numIter);
         for (int j = 0; j < w; j++) conv[j0 + j] = S->conv[j];
         CHK(phist_Dcarp_cgState_delete(S, &iflag));
       }
@@ -199,21 +204,21 @@ int main(int argc, char** argv)
   double maxres = 0.0;
   for (int j = 0; j < nshifts; j++) {
     nconv += conv[j];
-    maxres = std::max(maxres, relres[j]);
+    maxres = std::isfinite(relres[j]) ? std::max(maxres, relres[j]) : INFINITY;
   }
   printf("{\"problem\": \"%s\", \"mixed\": %d, \"innerTol\": %.3e, \"refinements\": [", problem, mixed,
          innerTol);
   for (size_t i = 0; i < refines.size(); i++) printf("%s%d", i ? ", " : "", refines[i]);
   printf("], \"n\": %d, \"nshifts\": %d, \"block\": %d, \"tol\": %.3e, \"maxIter\": %d, "
-         "\"omega\": %g, \"nconv\": %d, \"max_relres\": %.6e, \"launches\": %llu, \"iters\": [",
-         nloc, nshifts, block, tol, maxIter, omega, nconv, maxres, (unsigned long long)launches);
-  for (size_t i = 0; i < iters.size(); i++) printf("%s%d", i ? ", " : "", iters[i]);
-  printf("], \"wall\": [");
+         "\"omega\": %g, \"nconv\": %d, \"launches\": %llu, \"max_relres\": ",
+         nloc, nshifts, block, tol, maxIter, omega, nconv, (unsigned long long)launches);
+  jnum("", maxres, "%.6e");
+  printf(", \"wall\": [");
   for (size_t i = 0; i < walls.size(); i++) printf("%s%.6f", i ? ", " : "", walls[i]);
   printf("], \"shifts\": [");
   for (int j = 0; j < nshifts; j++) printf("%s%.17g", j ? ", " : "", shifts[j]);
   printf("], \"relres\": [");
-  for (int j = 0; j < nshifts; j++) printf("%s%.6e", j ? ", " : "", relres[j]);
+  for (int j = 0; j < nshifts; j++) jnum(j ? ", " : "", relres[j], "%.6e");
   printf("]}\n");
   fflush(stdout);
   if (!out.empty()) {

@@ -89,7 +89,7 @@ extern "C" void phist_b200_mixed_carp_create(pb_mixed_carp** out, void const* A,
 
 extern "C" void phist_b200_mixed_carp_solve(pb_mixed_carp* me, void const* B, void* X, const double omega[],
                                             double tol, double innerTol, int maxInnerIter, int maxRefine,
-                                            int* innerIters, int* refinements, int* iflag)
+                                            int* refinements, int* iflag)
 {
   *iflag = 0;
   if (!me || !B || !X) {
@@ -100,7 +100,7 @@ extern "C" void phist_b200_mixed_carp_solve(pb_mixed_carp* me, void const* B, vo
   for (int j = 0; j < ns; j++) me->S->omega_[j] = omega ? (float)omega[j] : 1.0f;
   std::vector<double> nb(ns), nr(ns);
   PB_CHK(phist_Dmvec_norm2((phist_Dconst_mvec_ptr)B, nb.data(), iflag));
-  int its = 0, k = 0, unconverged = ns;
+  int k = 0, unconverged = ns;
   for (;; k++) {
     // r = b - (A - sigma I) x in FP64
     PB_CHK(phist_Dmvec_add_mvec(1.0, (phist_Dconst_mvec_ptr)B, 0.0, me->R, iflag));
@@ -117,12 +117,10 @@ extern "C" void phist_b200_mixed_carp_solve(pb_mixed_carp* me, void const* B, vo
     *iflag = 0;
     phist_Scarp_cgState_iterate(me->S, me->Ds, nullptr, (float)innerTol, maxInnerIter, 0, iflag);
     if (*iflag < 0) return;
-    its += me->S->numIter;
     // x += d in FP64
     PB_CHK(phist_b200_mvec_StoD(me->Ds, me->D, iflag));
     PB_CHK(phist_Dmvec_add_mvec(1.0, me->D, 1.0, (phist_Dmvec_ptr)X, iflag));
   }
-  if (innerIters) *innerIters = its;
   if (refinements) *refinements = k;
   *iflag = unconverged;
 }

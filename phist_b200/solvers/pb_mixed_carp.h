@@ -31,12 +31,11 @@ void phist_b200_mixed_carp_create(pb_mixed_carp** me, void const* A, int nsys, c
 
 /* B, X: phist_Dmvec_ptr with nsys columns on A's row map; X holds the start
  * guess on entry.  omega[nsys] relaxation parameters (NULL: 1).  On exit
- * *innerIters is the total number of FP32 CARP-CG iterations, *refinements
- * the number of FP64 residual corrections; *iflag > 0 counts the systems that
- * did not reach tol within maxRefine corrections. */
+ * *refinements is the number of FP64 residual corrections; *iflag > 0 counts
+ * the systems that did not reach tol within maxRefine corrections. */
 void phist_b200_mixed_carp_solve(pb_mixed_carp* me, void const* B, void* X, const double omega[], double tol,
-                                 double innerTol, int maxInnerIter, int maxRefine, int* innerIters,
-                                 int* refinements, int* iflag);
+                                 double innerTol, int maxInnerIter, int maxRefine, int* refinements,
+                                 int* iflag);
 
 void phist_b200_mixed_carp_delete(pb_mixed_carp* me, int* iflag);
 
