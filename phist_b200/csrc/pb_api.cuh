@@ -5,6 +5,7 @@
 #pragma once
 #include <cudaTypedefs.h>
 #include <algorithm>
+#include <type_traits>
 #include <cmath>
 #include <numeric>
 
@@ -15,6 +16,7 @@
 #include "pb_spmmv.cuh"
 #include "pb_spmmv_staged.cuh"
 #include "pb_tile.cuh"
+#include "pb_dmma.cuh"
 
 namespace pb {
 
@@ -876,6 +878,30 @@ void mvtmv_async_launch(MvTmvArgs<T>& a, int64_t n)
   // many outputs: the cross-block sum as a second, GPU-wide pass
   const int nout = a.m * a.k;
   a.ext_reduce = (nout >= 64 && grid > 1) ? 1 : 0;
+  // FP64 on the tensor cores (DMMA) for widths that are multiples of 8
+  if constexpr (std::is_same<T, double>::value && BM >= 8 && BK >= 8) {
+    constexpr int DPV = BM + 4, DPW = BK + 4;
+    constexpr int DR0 = (4096 / (DPV + DPW)) / 32 * 32;
+    constexpr int DR = DR0 < 32 ? 32 : DR0 > 256 ? 256 : DR0;
+    CUtensorMap mV, mW;
+    if (rt().use_tma && rt().use_dmma && make_rows_tmap<T>(&mV, a.V, n, a.m, a.ldv, DPV, DR) &&
+        make_rows_tmap<T>(&mW, a.W, n, a.k, a.ldw, DPW, DR)) {
+      const size_t dsmem = sizeof(T) * (size_t)S * DR * (DPV + DPW) + 8 * S;
+      const int dgrid = (int)std::min<int64_t>(ceil_div(n, DR), (int64_t)rt().num_sms() * 2);
+      a.part = (T*)rt().scratch(sizeof(T) * (size_t)dgrid * a.m * a.k);
+      a.ext_reduce = (nout >= 64 && dgrid > 1) ? 1 : 0;
+      a.R = DR;
+      auto kd = k_mvtmv_dmma<BM, BK, DR, S>;
+      set_smem(kd, dsmem);
+      kd<<<dgrid, BLK_BS, dsmem, stream()>>>(a, mV, mW, rt().device_error_word());
+      if (a.ext_reduce) {
+        PB_LAUNCH_CHECK();
+        k_reduce_partials<T><<<(nout + 31) / 32, 256, 0, stream()>>>(a.part, dgrid, nout, a.Cd, a.m, a.ldc,
+                                                                      a.alpha, a.beta);
+      }
+      return;
+    }
+  }
   // TMA staging where both blocks can be described by tensor maps
   constexpr int RT = R > 256 ? 256 : R;
   CUtensorMap mapV, mapW;
@@ -1004,6 +1030,41 @@ void mvsd_async_launch(RowGemmArgs<T>& a)
   constexpr int S = (R * AP * (int)sizeof(T) > 30000) ? 3 : 4;
   const size_t smem = sizeof(T) * ((size_t)BM * BK + (size_t)S * R * AP);
   const int grid = (int)std::min<int64_t>(ceil_div(a.n > 0 ? a.n : 1, R), (int64_t)rt().num_sms() * 2);
+  if constexpr (std::is_same<T, double>::value && BM >= 8 && BK >= 8) {
+    // FP64 on the tensor cores (DMMA), rows staged by TMA
+    constexpr int DAP = BM + 4, DCP = BK + 4;
+    constexpr int DR = (DAP * 8 * 128 <= 24576) ? 128 : 64;
+    constexpr int DS = (DR * DAP * 8 > 30000) ? 3 : 4;
+    constexpr int DCSZ = (BM * DCP * 8 + 127) / 128 * 128 / 8;
+    const T* A = (a.mode == RM_MVSDI) ? (const T*)a.W : a.V;
+    const int64_t lda = (a.mode == RM_MVSDI) ? a.ldw : a.ldv;
+    CUtensorMap mA;
+    if (rt().use_tma && rt().use_dmma && make_rows_tmap<T>(&mA, A, a.n, a.m, lda, DAP, DR)) {
+      const size_t dsmem = sizeof(T) * ((size_t)DCSZ + (size_t)DS * DR * DAP) + 8 * DS;
+      const int dgrid = (int)std::min<int64_t>(ceil_div(a.n, DR), (int64_t)rt().num_sms() * 2);
+      auto kd = k_mvsd_dmma<BM, BK, DR, DS>;
+      set_smem(kd, dsmem);
+      kd<<<dgrid, BLK_BS, dsmem, stream()>>>(a, mA, rt().device_error_word());
+      return;
+    }
+  }
+  {
+    // TMA staging of the input rows where a tensor map describes them
+    constexpr int TRT = (TY * TR > 256) ? 256 / TY : TR;
+    constexpr int RT = TY * TRT;
+    const T* A = (a.mode == RM_MVSDI) ? (const T*)a.W : a.V;
+    const int64_t lda = (a.mode == RM_MVSDI) ? a.ldw : a.ldv;
+    CUtensorMap mapA;
+    if (rt().use_tma && make_rows_tmap<T>(&mapA, A, a.n, a.m, lda, AP, RT)) {
+      constexpr int CSZ = (BM * BK * (int)sizeof(T) + 127) / 128 * 128 / (int)sizeof(T);
+      const size_t tsmem = sizeof(T) * ((size_t)CSZ + (size_t)S * RT * AP) + 8 * S;
+      const int tgrid = (int)std::min<int64_t>(ceil_div(a.n, RT), (int64_t)rt().num_sms() * 2);
+      auto kt = k_mvsd_tma<T, BM, BK, TRT, TC, S>;
+      set_smem(kt, tsmem);
+      kt<<<tgrid, BLK_BS, tsmem, stream()>>>(a, mapA, rt().device_error_word());
+      return;
+    }
+  }
   auto kern = k_mvsd_async<T, BM, BK, TR, TC, S>;
   set_smem(kern, smem);
   kern<<<grid, BLK_BS, smem, stream()>>>(a);

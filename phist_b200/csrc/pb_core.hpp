@@ -163,6 +163,8 @@ class Runtime {
   int spmv_staged_min_nvec = 99;
   // stage block-vector tiles of the Gram kernels with TMA (else cp.async)
   bool use_tma = true;
+  // FP64 block products on the tensor cores (DMMA) for widths multiple of 8
+  bool use_dmma = true;
 
   // statistics: kernel launches issued by this library
   uint64_t launches = 0;

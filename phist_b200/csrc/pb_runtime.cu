@@ -45,6 +45,7 @@ void Runtime::init()
   memset(mbox_h_, 0, kMailboxBytes);
   if (const char* v = getenv("PHIST_B200_VERBOSE")) verbose = atoi(v);
   if (const char* v = getenv("PHIST_B200_TMA")) use_tma = atoi(v) != 0;
+  if (const char* v = getenv("PHIST_B200_DMMA")) use_dmma = atoi(v) != 0;
   if (const char* c = getenv("PHIST_B200_SELL_C")) sell_C = atoi(c);
   if (const char* s = getenv("PHIST_B200_SELL_SIGMA")) sell_sigma_default = atoll(s);
   inited_ = true;

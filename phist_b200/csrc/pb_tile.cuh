@@ -333,4 +333,103 @@ __global__ void __launch_bounds__(256) k_mvsd_async(RowGemmArgs<T> a)
   cp_async_wait<0>();
 }
 
+// ------------------------------------------------------------ V*C, TMA-staged
+// k_mvsd_async with the input row tiles delivered as 2D TMA boxes (R rows x
+// AP columns, zero-filled past m) on per-stage mbarriers; thread mapping,
+// output writes and the in-place rule are those of k_mvsd_async.
+template <class T, int BM, int BK, int TR, int TC, int S>
+__global__ void __launch_bounds__(256) k_mvsd_tma(RowGemmArgs<T> a, const __grid_constant__ CUtensorMap mapA,
+                                                  int* err)
+{
+  constexpr int TX = BK / TC, TY = 256 / TX, R = TY * TR;
+  constexpr int AP = BM + 16 / sizeof(T);
+  constexpr unsigned STAGE_BYTES = (unsigned)(R * AP * sizeof(T));
+  // sC padded to 128 bytes: TMA destinations start on 128-byte boundaries
+  constexpr int CSZ = (BM * BK * (int)sizeof(T) + 127) / 128 * 128 / (int)sizeof(T);
+  static_assert(S >= 2 && TX * TY == 256 && R <= 256, "bad tile shape");
+  extern __shared__ __align__(128) unsigned char smem_raw[];
+  T* sC = reinterpret_cast<T*>(smem_raw);  // [BM][BK]
+  T* sA = sC + CSZ;                         // [S][R][AP]
+  uint64_t* bar = reinterpret_cast<uint64_t*>(sA + S * R * AP);
+  const int tid = threadIdx.x;
+  const int ty = tid / TX, tx = tid - ty * TX;
+  const bool inplace = (a.mode == RM_MVSDI);
+  const int64_t ntiles = (a.n + R - 1) / R;
+
+  if (tid == 0) {
+    for (int st = 0; st < S; st++) mbar_init(&bar[st], 1);
+    mbar_fence_init();
+    tma_prefetch_desc(&mapA);
+  }
+  for (int q = tid; q < BM * BK; q += blockDim.x) sC[q] = T(0);
+  __syncthreads();
+  for (int q = tid; q < a.m * a.k; q += blockDim.x) {
+    const int i = q % a.m, j = q / a.m;
+    sC[i * BK + j] = a.C[i + j * a.ldc];
+  }
+  if (tid == 0) {
+    for (int st = 0; st < S - 1; st++) {
+      const int64_t tl = blockIdx.x + (int64_t)st * gridDim.x;
+      if (tl < ntiles) {
+        mbar_arrive_expect_tx(&bar[st], STAGE_BYTES);
+        tma_load_2d(sA + st * R * AP, &mapA, 0, (int)(tl * R), &bar[st]);
+      }
+    }
+  }
+  __syncthreads();  // sC complete
+
+  T out[TR][TC];
+  bool ok = true;
+  int stage = 0;
+  int64_t it = 0;
+  for (int64_t tile = blockIdx.x; tile < ntiles; tile += gridDim.x, it++) {
+    if (tid == 0) {
+      const int64_t nt = tile + (int64_t)(S - 1) * gridDim.x;
+      const int ps = (stage + S - 1) % S;
+      if (nt < ntiles) {
+        mbar_arrive_expect_tx(&bar[ps], STAGE_BYTES);
+        tma_load_2d(sA + ps * R * AP, &mapA, 0, (int)(nt * R), &bar[ps]);
+      }
+    }
+    const bool landed = mbar_wait(&bar[stage], (unsigned)((it / S) & 1), err);
+    ok = ok && landed;
+    if (ok) {
+      const T* a0 = sA + stage * R * AP;
+#pragma unroll
+      for (int p = 0; p < TR; p++)
+#pragma unroll
+        for (int q = 0; q < TC; q++) out[p][q] = T(0);
+#pragma unroll 4
+      for (int i = 0; i < BM; i++) {
+        T v[TR], c[TC];
+#pragma unroll
+        for (int p = 0; p < TR; p++) v[p] = a0[(ty + TY * p) * AP + i];
+#pragma unroll
+        for (int q = 0; q < TC; q++) c[q] = sC[i * BK + tx + TX * q];
+#pragma unroll
+        for (int p = 0; p < TR; p++)
+#pragma unroll
+          for (int q = 0; q < TC; q++) out[p][q] += v[p] * c[q];
+      }
+      const int64_t r0 = tile * R;
+#pragma unroll
+      for (int p = 0; p < TR; p++) {
+        const int64_t row = r0 + ty + TY * p;
+        if (row >= a.n) continue;
+        T* wr = a.W + row * a.ldw;
+#pragma unroll
+        for (int q = 0; q < TC; q++) {
+          const int j = tx + TX * q;
+          if (j < a.k) {
+            if (inplace) wr[j] = out[p][q];
+            else wr[j] = (a.beta != T(0)) ? a.alpha * out[p][q] + a.beta * wr[j] : a.alpha * out[p][q];
+          }
+        }
+      }
+    }
+    __syncthreads();
+    stage = (stage + 1) % S;
+  }
+}
+
 }  // namespace pb

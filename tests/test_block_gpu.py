@@ -9,7 +9,8 @@ from conftest import relerr
 pytestmark = pytest.mark.gpu
 TOL = 1e-13
 
-SHAPES = [(1, 1), (2, 3), (4, 4), (5, 7), (8, 8), (4, 40), (40, 4), (16, 16), (32, 32), (64, 64), (13, 29)]
+SHAPES = [(1, 1), (2, 3), (4, 4), (5, 7), (8, 8), (4, 40), (40, 4), (16, 16), (32, 32), (64, 64), (13, 29),
+          (24, 8), (8, 24), (64, 16), (16, 64), (40, 56)]
 
 
 def _mk(n, ncol, data, dtype=np.float64):
