@@ -369,8 +369,8 @@ void phist_b200_DmvecT_times_mvec_noalloc(int64_t n, int m, int k, double alpha,
  * matrix is built with PHIST_SPARSEMAT_PERM_LOCAL (<=1: no sorting) */
 void phist_b200_set_sell_params(int C, int64_t sigma, int* iflag);
 /* SpMMV launch shape (autotuning control): threads per matrix row for block
- * width nvec (1,2,4,8,16,32; allowed pairs 1:1, 2:1, 4:1|2, 8:2|4, 16:4|8,
- * 32:8|16) and, when unroll >= 0, whether the fully unrolled kernel for
+ * width nvec (1,2,4,8,16,32; allowed 1:1, 2:1, 4:1|2, 8:1|2|4, 16:2|4|8,
+ * 32:4|8|16) and, when unroll >= 0, whether the fully unrolled kernel for
  * matrices whose rows have at most 8 entries may be used */
 void phist_b200_set_spmv_config(int nvec, int tpr, int unroll, int* iflag);
 /* block widths >= min_nvec (8..32) use the SpMMV kernel that stages the

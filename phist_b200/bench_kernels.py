@@ -104,7 +104,7 @@ def suite_spmmv_tune(T, reps, peak, L=128):
     K.chk(K.phist_b200_set_sell_params, 32, 256)
     A = SparseMat.from_problem("ANDERSON3D-%d-S1" % L, flags=K.PHIST_SPARSEMAT_PERM_LOCAL)
     n, nnz = A.nrows, A.nnz
-    opts = {1: (1,), 2: (1,), 4: (1, 2), 8: (2, 4), 16: (4, 8), 32: (8, 16)}
+    opts = {1: (1,), 2: (1,), 4: (1, 2), 8: (1, 2, 4), 16: (2, 4, 8), 32: (4, 8, 16)}
     out = []
     for nv, tprs in opts.items():
         X = Mvec(A.domain_map, nv).set(random_block(n, nv, 3))

@@ -714,14 +714,17 @@ void spmv_tile(const SparseMat<T>* A, SpmvArgs<T>& p, int nv)
       break;
     case 8:
       if (tpr == 4) launch_spmv_nv<T, 8, 4>(A, S, p, vec);
+      else if (tpr == 1) launch_spmv_nv<T, 8, 1>(A, S, p, vec);
       else launch_spmv_nv<T, 8, 2>(A, S, p, vec);
       break;
     case 16:
       if (tpr == 8) launch_spmv_nv<T, 16, 8>(A, S, p, vec);
+      else if (tpr == 2) launch_spmv_nv<T, 16, 2>(A, S, p, vec);
       else launch_spmv_nv<T, 16, 4>(A, S, p, vec);
       break;
     default:
       if (tpr == 16) launch_spmv_nv<T, 32, 16>(A, S, p, vec);
+      else if (tpr == 4) launch_spmv_nv<T, 32, 4>(A, S, p, vec);
       else launch_spmv_nv<T, 32, 8>(A, S, p, vec);
       break;
   }

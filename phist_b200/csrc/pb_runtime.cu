@@ -443,14 +443,14 @@ void phist_b200_set_sell_params(int C, int64_t sigma, int* iflag)
 void phist_b200_set_spmv_config(int nvec, int tpr, int unroll, int* iflag)
 {
   PB_API_BEGIN(iflag);
-  static const int allowed[6][2] = {{1, 1}, {1, 1}, {1, 2}, {2, 4}, {4, 8}, {8, 16}};
+  static const int allowed[6][3] = {{1, 1, 1}, {1, 1, 1}, {1, 2, 2}, {1, 2, 4}, {2, 4, 8}, {4, 8, 16}};
   int lg = -1;
   for (int q = 0; q < 6; q++)
     if (nvec == (1 << q)) lg = q;
   PB_REQUIRE(lg >= 0, PB_INVALID_INPUT, "nvec must be 1,2,4,8,16 or 32, got %d", nvec);
-  PB_REQUIRE(tpr == allowed[lg][0] || tpr == allowed[lg][1], PB_INVALID_INPUT,
-             "threads per row %d not available for nvec %d (use %d or %d)", tpr, nvec,
-             allowed[lg][0], allowed[lg][1]);
+  PB_REQUIRE(tpr == allowed[lg][0] || tpr == allowed[lg][1] || tpr == allowed[lg][2], PB_INVALID_INPUT,
+             "threads per row %d not available for nvec %d (use %d, %d or %d)", tpr, nvec,
+             allowed[lg][0], allowed[lg][1], allowed[lg][2]);
   rt().spmv_tpr[lg] = tpr;
   if (unroll >= 0) rt().spmv_unroll = unroll != 0;
   PB_API_END(iflag);

@@ -68,6 +68,10 @@ struct VecLd<double, 2> {
     double2 v = *reinterpret_cast<const double2*>(p);
     o[0] = v.x; o[1] = v.y;
   }
+  static __device__ __forceinline__ void ld_ordered(const double* p, double* o)
+  {
+    asm volatile("ld.global.nc.v2.f64 {%0, %1}, [%2];\n" : "=d"(o[0]), "=d"(o[1]) : "l"(p));
+  }
   static __device__ __forceinline__ void st(double* p, const double* o)
   {
     *reinterpret_cast<double2*>(p) = make_double2(o[0], o[1]);
@@ -84,6 +88,12 @@ struct VecLd<float, 4> {
   {
     float4 v = *reinterpret_cast<const float4*>(p);
     o[0] = v.x; o[1] = v.y; o[2] = v.z; o[3] = v.w;
+  }
+  static __device__ __forceinline__ void ld_ordered(const float* p, float* o)
+  {
+    asm volatile("ld.global.nc.v4.f32 {%0, %1, %2, %3}, [%4];\n"
+                 : "=f"(o[0]), "=f"(o[1]), "=f"(o[2]), "=f"(o[3])
+                 : "l"(p));
   }
   static __device__ __forceinline__ void st(float* p, const float* o)
   {
@@ -102,14 +112,29 @@ struct VecLd<float, 2> {
     float2 v = *reinterpret_cast<const float2*>(p);
     o[0] = v.x; o[1] = v.y;
   }
+  static __device__ __forceinline__ void ld_ordered(const float* p, float* o)
+  {
+    asm volatile("ld.global.nc.v2.f32 {%0, %1}, [%2];\n" : "=f"(o[0]), "=f"(o[1]) : "l"(p));
+  }
   static __device__ __forceinline__ void st(float* p, const float* o)
   {
     *reinterpret_cast<float2*>(p) = make_float2(o[0], o[1]);
   }
 };
+__device__ __forceinline__ void ld_ordered1(const double* p, double* o)
+{
+  asm volatile("ld.global.nc.f64 %0, [%1];\n" : "=d"(o[0]) : "l"(p));
+}
+__device__ __forceinline__ void ld_ordered1(const float* p, float* o)
+{
+  asm volatile("ld.global.nc.f32 %0, [%1];\n" : "=f"(o[0]) : "l"(p));
+}
+__device__ __forceinline__ void reg_fence(double& v) { asm volatile("" : "+d"(v)); }
+__device__ __forceinline__ void reg_fence(float& v) { asm volatile("" : "+f"(v)); }
 template <class T>
 struct VecLd1 {
   static __device__ __forceinline__ void ld(const T* p, T* o) { o[0] = __ldg(p); }
+  static __device__ __forceinline__ void ld_ordered(const T* p, T* o) { ld_ordered1(p, o); }
   static __device__ __forceinline__ void ld_plain(const T* p, T* o) { o[0] = *p; }
   static __device__ __forceinline__ void st(T* p, const T* o) { *p = o[0]; }
 };
@@ -204,6 +229,12 @@ k_sell_spmmv(SellDev<T> A, SpmvArgs<T> p)
         cv[k] = __ldcs(A.col + base + (int64_t)k * C);
       }
     }
+    // entries past the chunk length gather the row of entry 0 again (an L1
+    // hit) and are not accumulated: the gathers carry no predicate and can
+    // all be issued before the first one is consumed
+#pragma unroll
+    for (int k = 1; k < KMAX; k++)
+      if (k >= len) cv[k] = cv[0];
     T xv[KMAX > 0 ? KMAX : 1][VPT];
 #pragma unroll
     for (int k = 0; k < KMAX; k++) {
@@ -211,11 +242,20 @@ k_sell_spmmv(SellDev<T> A, SpmvArgs<T> p)
 #pragma unroll
       for (int v = 0; v < NVV; v++) {
         const int c = spmv_col<TPR, VW>(s, v, 0);
+        if (VEC || c < nv) {
+          Vec<T, VW>::ld_ordered(xr + c, &xv[k][v * VW]);
+        } else {
 #pragma unroll
-        for (int w = 0; w < VW; w++) xv[k][v * VW + w] = T(0);
-        if (k < len && (VEC || c < nv)) Vec<T, VW>::ld(xr + c, &xv[k][v * VW]);
+          for (int w = 0; w < VW; w++) xv[k][v * VW + w] = T(0);
+        }
       }
     }
+    // compiler fence: every gathered value is an operand here, so the
+    // accumulation below cannot be interleaved with (and wait on) the loads
+#pragma unroll
+    for (int k = 0; k < KMAX; k++)
+#pragma unroll
+      for (int q = 0; q < VPT; q++) reg_fence(xv[k][q]);
 #pragma unroll
     for (int k = 0; k < KMAX; k++)
       if (k < len)

@@ -279,6 +279,37 @@ def test_staged_kernel_matches_oracle_and_register_path(session, oracle, prob, n
     X.delete(); Y.delete(); A.delete()
 
 
+@pytest.mark.parametrize("nvec,tprs", [(4, (1, 2)), (8, (1, 2, 4)), (16, (2, 4, 8)), (32, (4, 8, 16))])
+@pytest.mark.parametrize("prob", ["LAPDIAG3D-12-S5", "HONEYCOMB-20-S4-W1"])
+def test_every_launch_shape_matches_oracle(session, oracle, prob, nvec, tprs):
+    """every threads-per-row choice of phist_b200_set_spmv_config, unrolled
+    (rows of at most 8 entries) and runtime-loop kernels, against the oracle"""
+    from phist_b200 import generators as G
+    from phist_b200 import kernels as K
+    from phist_b200.objects import Mvec, SparseMat
+    K.chk(K.phist_b200_set_sell_params, 32, 256)
+    rp, c, v = G.problem(prob)
+    A = SparseMat.from_crs(rp, c, v, flags=K.PHIST_SPARSEMAT_PERM_LOCAL)
+    n = len(rp) - 1
+    x = G.random_block(n, nvec, 11)
+    y0 = G.random_block(n, nvec, 12)
+    sh = np.linspace(-1, 1, nvec)
+    X = Mvec(A.domain_map, nvec).set(x)
+    Y = Mvec(A.row_map, nvec)
+    ref = oracle.spmmv(rp, c, v, x, alpha=0.75, beta=-0.5, y=y0, shifts=sh)
+    defaults = {4: 1, 8: 2, 16: 4, 32: 8}
+    try:
+        for tpr in tprs:
+            for unroll in (1, 0):
+                K.chk(K.phist_b200_set_spmv_config, nvec, tpr, unroll)
+                Y.set(y0)
+                K.chk(K.phist_DsparseMat_times_mvec_vadd_mvec, 0.75, A.h, K.sptr(sh, np.float64), X.h, -0.5, Y.h)
+                assert relerr(Y.get(), ref) < TOL, (tpr, unroll)
+    finally:
+        K.chk(K.phist_b200_set_spmv_config, nvec, defaults[nvec], 1)
+    X.delete(); Y.delete(); A.delete()
+
+
 def test_read_mm(session, oracle, testmats, tmp_path):
     """sparseMat_read_mm (phist_kernels_decl.h:98) on a MatrixMarket file"""
     import ctypes as ct
