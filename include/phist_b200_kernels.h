@@ -364,6 +364,25 @@ void phist_b200_DmvecT_times_mvec_noalloc(int64_t n, int m, int k, double alpha,
                                           const double* W, int64_t ldw, double beta,
                                           double* C, int64_t ldc, void* stream, int* iflag);
 
+/* Batched multi-shift CARP-CG (library extension; the solver behind PHIST's
+ * carp_cg driver, drivers/carp_cg.c:286-320, with the CGMN recurrence of
+ * src/krylov/phist_carp_cg_def.hpp:440-690 run on the GPU).  Solves
+ * (A - sigma_j I) x_j = b_j for the nsys columns of B (n x nsys) into X
+ * (n x nsys) through `block` (1..32) slots: each slot iterates one system;
+ * every checkEvery iterations the explicit FP64 residuals are measured, and
+ * a system that reached ||b_j - (A - sigma_j I) x_j|| <= tol ||b_j|| (or
+ * maxIter iterations) leaves its slot to the next queued system.  All CG
+ * scalars live on the device; an iteration synchronises with the host only
+ * at the checks.  mixed = 1: FP32 sweeps and FP32 CG on an FP32 copy of A,
+ * inside per-slot FP64 iterative refinement (inner relative tolerance
+ * innerTol, <= 0 selects 1e-5).  On exit iters[j] holds the CG iterations
+ * spent on system j and relres[j] its final FP64 relative residual;
+ * *iflag >= 0 is the number of systems that did not reach tol. */
+void phist_b200_DcarpCG_batch(phist_Dconst_sparseMat_ptr A, int nsys, const double sigma[],
+                              phist_Dconst_mvec_ptr B, phist_Dmvec_ptr X, int block, double tol,
+                              int maxIter, int checkEvery, int mixed, double innerTol, int iters[],
+                              double relres[], int* iflag);
+
 /* runtime controls and statistics (library extensions) */
 /* SELL chunk height C (1..32, power of two) and the sigma window used when a
  * matrix is built with PHIST_SPARSEMAT_PERM_LOCAL (<=1: no sorting) */

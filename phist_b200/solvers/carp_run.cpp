@@ -19,6 +19,10 @@
 //         mixed=1: FP32 CARP-CG inside FP64 iterative refinement
 //         (pb_mixed_carp.h) with innerTol (1e-5) and maxRefine (20); maxIter
 //         then bounds the FP32 iterations of each refinement step
+//         batch=1: the library's batched solver phist_b200_DcarpCG_batch
+//         instead of PHIST's carp_cgState (block = slots, converged systems
+//         refilled from the queue, checks every checkEvery (10) iterations;
+//         mixed=1 there means FP32 inner solves with FP64 refinement)
 //   shifts sigma_j = 2.5 * u(seed, j), right-hand sides b_ij = u(seed + 1 + j, i)
 //   with u uniform [-1,1) from a splitmix64 hash (the library's pb_unif).
 #include <algorithm>
@@ -43,6 +47,10 @@ void phist_b200_Dcreate_problem(phist_DsparseMat_ptr* A, phist_const_comm_ptr co
 void phist_b200_set_sell_params(int C, int64_t sigma, int* iflag);
 void phist_b200_synchronize(int* iflag);
 void phist_b200_launch_count(uint64_t* count, int* iflag);
+void phist_b200_DcarpCG_batch(phist_Dconst_sparseMat_ptr A, int nsys, const double sigma[],
+                              phist_Dconst_mvec_ptr B, phist_Dmvec_ptr X, int block, double tol,
+                              int maxIter, int checkEvery, int mixed, double innerTol, int iters[],
+                              double relres[], int* iflag);
 }
 
 #define CHK(call)                                                              \
@@ -88,7 +96,7 @@ int main(int argc, char** argv)
   uint64_t seed = 4;
   int64_t sigma = 1;
   std::string out;
-  int mixed = 0, maxRefine = 20;
+  int mixed = 0, maxRefine = 20, batch = 0, checkEvery = 10;
   double innerTol = 1e-5;
   for (int a = 2; a < argc; a++) {
     const char* kv = argv[a];
@@ -108,6 +116,8 @@ int main(int argc, char** argv)
     else if (k == "mixed") mixed = atoi(v);
     else if (k == "innerTol") innerTol = atof(v);
     else if (k == "maxRefine") maxRefine = atoi(v);
+    else if (k == "batch") batch = atoi(v);
+    else if (k == "checkEvery") checkEvery = atoi(v);
   }
   if (block < 1 || nshifts < 1) return 2;
 
@@ -138,7 +148,7 @@ int main(int argc, char** argv)
   }
 
   std::vector<double> walls, relres(nshifts, 0.0);
-  std::vector<int> refines, conv(nshifts, 0);
+  std::vector<int> refines, conv(nshifts, 0), batch_iters;
   uint64_t launches = 0;
   for (int rep = 0; rep < reps; rep++) {
     CHK(phist_Dmvec_put_value(X, 0.0, &iflag));
@@ -147,7 +157,18 @@ int main(int argc, char** argv)
     CHK(phist_b200_launch_count(&l0, &iflag));
     CHK(phist_b200_synchronize(&iflag));
     auto t0 = std::chrono::steady_clock::now();
-    for (int j0 = 0; j0 < nshifts; j0 += block) {
+    if (batch) {
+      std::vector<double> brel(nshifts, 0.0);
+      batch_iters.assign(nshifts, 0);
+      iflag = 0;
+      phist_b200_DcarpCG_batch(A, nshifts, shifts.data(), B, X, block, tol, maxIter, checkEvery, mixed, innerTol,
+                               batch_iters.data(), brel.data(), &iflag);
+      if (iflag < 0) {
+        fprintf(stderr, "DcarpCG_batch returned %d\n", iflag);
+        return 1;
+      }
+    }
+    for (int j0 = 0; j0 < nshifts && !batch; j0 += block) {
       const int w = std::min(block, nshifts - j0);
       phist_Dmvec_ptr Bj = NULL, Xj = NULL;
       CHK(phist_Dmvec_view_block(B, &Bj, j0, j0 + w - 1, &iflag));
@@ -196,8 +217,8 @@ int main(int argc, char** argv)
     CHK(phist_Dmvec_norm2(B, nb.data(), &iflag));
     CHK(phist_Dmvec_norm2(R, nr.data(), &iflag));
     for (int j = 0; j < nshifts; j++) relres[j] = nr[j] / nb[j];
-    // the refinement loop stops on exactly this FP64 residual test
-    if (mixed)
+    // the refinement loops stop on exactly this FP64 residual test
+    if (mixed || batch)
       for (int j = 0; j < nshifts; j++) conv[j] = nr[j] <= tol * nb[j];
   }
   int nconv = 0;
@@ -213,7 +234,9 @@ int main(int argc, char** argv)
          "\"omega\": %g, \"nconv\": %d, \"launches\": %llu, \"max_relres\": ",
          nloc, nshifts, block, tol, maxIter, omega, nconv, (unsigned long long)launches);
   jnum("", maxres, "%.6e");
-  printf(", \"wall\": [");
+  printf(", \"batch\": %d, \"batch_iters\": [", batch);
+  for (size_t i = 0; i < batch_iters.size(); i++) printf("%s%d", i ? ", " : "", batch_iters[i]);
+  printf("], \"wall\": [");
   for (size_t i = 0; i < walls.size(); i++) printf("%s%.6f", i ? ", " : "", walls[i]);
   printf("], \"shifts\": [");
   for (int j = 0; j < nshifts; j++) printf("%s%.17g", j ? ", " : "", shifts[j]);
