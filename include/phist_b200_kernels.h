@@ -397,6 +397,13 @@ void phist_b200_set_spmv_config(int nvec, int tpr, int unroll, int* iflag);
 void phist_b200_set_spmv_staged(int min_nvec, int* iflag);
 /* wait for all work this library enqueued */
 void phist_b200_synchronize(int* iflag);
+/* Every host thread that calls the library works on its own lane: a CUDA
+ * stream with its own scratch, counters, result mailbox and device-memory
+ * cache, so solves driven from several threads overlap on the GPU.  Objects
+ * are meant to be used by the thread that created them (read-only matrices
+ * may be shared).  phist_b200_synchronize drains the calling thread's lane;
+ * phist_b200_get_stream returns it.  Number of lanes created so far: */
+void phist_b200_lane_count(int* nlanes, int* iflag);
 /* number of kernel launches this library has issued since init */
 void phist_b200_launch_count(uint64_t* count, int* iflag);
 /* the CUDA stream all kernels are enqueued on (cudaStream_t) */

@@ -513,6 +513,9 @@ SparseMat<T>* build_sparse(const Comm* comm, int64_t nrows, int64_t ncols,
   A->h_col = std::move(col);
   A->h_val = std::move(val);
   A->h_perm = std::move(perm);
+  // the uploads ran on the creating thread's lane: drain it, so that the
+  // (read-only) matrix can be used from any thread's lane right away
+  rt().sync();
   return A;
 }
 

@@ -25,6 +25,7 @@
 #include <cstdio>
 #include <cstdlib>
 #include <cstring>
+#include <atomic>
 #include <map>
 #include <mutex>
 #include <stdexcept>
@@ -107,45 +108,70 @@ void report(const char* fcn, const char* msg);
   }
 
 // ---------------------------------------------------------------- runtime
-// Device memory cache: blocks freed by objects are kept per rounded size and
-// handed out again (solvers create and delete temporaries inside their
-// iterations; cudaMalloc/cudaFree would synchronise the device each time).
-// All kernels run in stream order on one stream, so a block freed after a
-// kernel was enqueued may be reused by the next kernel without a sync.
+// Lanes: every host thread that calls the library gets its own lane -- a
+// CUDA stream with its own reduction scratch, arrival counters, result
+// mailbox and device-memory cache -- so independent solves driven from
+// several host threads overlap on the GPU without sharing any mutable
+// device state.  A thread's lane is created on its first call and returned
+// to a pool (after its stream drained) when the thread exits.  Objects
+// (mvecs, sdMats, matrices) are meant to be used by one thread; matrices
+// that are only read may be shared.
+//
+// Device memory cache: blocks freed by objects are kept per rounded size in
+// the freeing thread's lane and handed out again to that lane only.  Its
+// kernels run in stream order on one stream, so a block freed after a kernel
+// was enqueued may be reused by the next kernel without a sync.
+struct Lane {
+  cudaStream_t stream = nullptr;
+  void* scratch = nullptr;
+  size_t scratch_bytes = 0;
+  unsigned int* counters = nullptr;  // 64 zero-initialised counters
+  void* mbox_h = nullptr;            // pinned, device-mapped result mailbox
+  void* mbox_d = nullptr;
+  std::multimap<size_t, void*> free_blocks;  // guarded by the runtime mutex
+  bool in_use = false;
+  unsigned generation = 0;
+};
+
 class Runtime {
  public:
   static Runtime& get();
   void init();
   void finalize();
   bool initialized() const { return inited_; }
-  cudaStream_t stream() const { return stream_; }
+  cudaStream_t stream() { return lane().stream; }
   int device() const { return device_; }
   int num_sms() const { return num_sms_; }
+
+  // the calling thread's lane (created or taken from the pool on first use)
+  Lane& lane();
+  void release_lane(Lane* l, unsigned generation);
+  int lanes_created() const { return (int)lanes_.size(); }
 
   void* dmalloc(size_t bytes);
   void dfree(void* p);
   void* hmalloc_pinned(size_t bytes);
   void hfree_pinned(void* p);
-  void sync();
+  void sync();  // drains the calling thread's lane
 
   // reusable device scratch for multi-block reductions: partial results per
   // block plus one arrival counter per launch (kept zero between launches)
   void* scratch(size_t bytes);
-  unsigned int* counters();  // 64 zero-initialised counters
+  unsigned int* counters();
 
-  // Result mailbox: kMailboxBytes of pinned host memory mapped into the
-  // device address space.  Calls that return values to the host (dots,
-  // norms, Gram matrices) have their final kernel or copy write here and
-  // read it after one stream synchronisation, with no pageable staging copy.
-  // One stream and one host thread use it, one call at a time.
+  // Result mailbox (per lane): kMailboxBytes of pinned host memory mapped
+  // into the device address space.  Calls that return values to the host
+  // (dots, norms, Gram matrices) have their final kernel or copy write here
+  // and read it after one stream synchronisation, with no pageable staging
+  // copy.  One call at a time per lane.
   static constexpr size_t kMailboxBytes = 1u << 20;
   // results use the first kMailboxResultBytes; the last 64 bytes hold the
   // device error word (kernels with bounded waits store a code there, and
   // sync() reports and clears it)
   static constexpr size_t kMailboxResultBytes = kMailboxBytes - 64;
-  void* mailbox_host() { if (!inited_) init(); return mbox_h_; }
-  void* mailbox_dev() { if (!inited_) init(); return mbox_d_; }
-  int* device_error_word() { if (!inited_) init(); return (int*)((char*)mbox_d_ + kMailboxResultBytes); }
+  void* mailbox_host() { return lane().mbox_h; }
+  void* mailbox_dev() { return lane().mbox_d; }
+  int* device_error_word() { return (int*)((char*)lane().mbox_d + kMailboxResultBytes); }
 
   // SELL parameters used for new matrices (C chunk height, sigma window)
   int sell_C = 32;
@@ -166,23 +192,20 @@ class Runtime {
   // FP64 block products on the tensor cores (DMMA) for widths multiple of 8
   bool use_dmma = true;
 
-  // statistics: kernel launches issued by this library
-  uint64_t launches = 0;
+  // statistics: kernel launches issued by this library (all lanes)
+  std::atomic<uint64_t> launches{0};
 
  private:
   Runtime() = default;
+  Lane* create_lane_locked();
+  void free_lane_locked(Lane* l);
   bool inited_ = false;
+  unsigned generation_ = 1;
   int device_ = 0;
   int num_sms_ = 148;
-  cudaStream_t stream_ = nullptr;
   std::mutex mu_;
-  std::multimap<size_t, void*> free_blocks_;
+  std::vector<Lane*> lanes_;
   std::map<void*, size_t> live_blocks_;
-  void* scratch_ = nullptr;
-  size_t scratch_bytes_ = 0;
-  unsigned int* counters_ = nullptr;
-  void* mbox_h_ = nullptr;
-  void* mbox_d_ = nullptr;
 };
 
 inline Runtime& rt() { return Runtime::get(); }

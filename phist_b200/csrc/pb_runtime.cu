@@ -36,13 +36,6 @@ void Runtime::init()
   cudaDeviceProp prop;
   PB_CUDA(cudaGetDeviceProperties(&prop, device_));
   num_sms_ = prop.multiProcessorCount;
-  PB_CUDA(cudaStreamCreateWithFlags(&stream_, cudaStreamNonBlocking));
-  PB_CUDA(cudaMalloc(&counters_, 64 * sizeof(unsigned int)));
-  PB_CUDA(cudaMemset(counters_, 0, 64 * sizeof(unsigned int)));
-  // pinned, device-mapped result buffer for calls that return host data
-  PB_CUDA(cudaHostAlloc(&mbox_h_, kMailboxBytes, cudaHostAllocMapped));
-  PB_CUDA(cudaHostGetDevicePointer(&mbox_d_, mbox_h_, 0));
-  memset(mbox_h_, 0, kMailboxBytes);
   if (const char* v = getenv("PHIST_B200_VERBOSE")) verbose = atoi(v);
   if (const char* v = getenv("PHIST_B200_TMA")) use_tma = atoi(v) != 0;
   if (const char* v = getenv("PHIST_B200_DMMA")) use_dmma = atoi(v) != 0;
@@ -51,24 +44,90 @@ void Runtime::init()
   inited_ = true;
 }
 
+Lane* Runtime::create_lane_locked()
+{
+  PB_CUDA(cudaSetDevice(device_));
+  Lane* l = new Lane();
+  PB_CUDA(cudaStreamCreateWithFlags(&l->stream, cudaStreamNonBlocking));
+  PB_CUDA(cudaMalloc(&l->counters, 64 * sizeof(unsigned int)));
+  PB_CUDA(cudaMemset(l->counters, 0, 64 * sizeof(unsigned int)));
+  PB_CUDA(cudaHostAlloc(&l->mbox_h, kMailboxBytes, cudaHostAllocMapped));
+  PB_CUDA(cudaHostGetDevicePointer(&l->mbox_d, l->mbox_h, 0));
+  memset(l->mbox_h, 0, kMailboxBytes);
+  l->generation = generation_;
+  return l;
+}
+
+void Runtime::free_lane_locked(Lane* l)
+{
+  if (l->stream) cudaStreamSynchronize(l->stream);
+  for (auto& kv : l->free_blocks) cudaFree(kv.second);
+  l->free_blocks.clear();
+  if (l->scratch) cudaFree(l->scratch);
+  if (l->counters) cudaFree(l->counters);
+  if (l->mbox_h) cudaFreeHost(l->mbox_h);
+  if (l->stream) cudaStreamDestroy(l->stream);
+  l->scratch = nullptr;
+  l->scratch_bytes = 0;
+  l->counters = nullptr;
+  l->mbox_h = l->mbox_d = nullptr;
+  l->stream = nullptr;
+}
+
+namespace {
+// the calling thread's lane; returned to the pool when the thread exits
+struct LaneHolder {
+  Lane* lane = nullptr;
+  unsigned generation = 0;
+  ~LaneHolder()
+  {
+    if (lane) Runtime::get().release_lane(lane, generation);
+  }
+};
+thread_local LaneHolder tl_lane;
+}  // namespace
+
+Lane& Runtime::lane()
+{
+  if (tl_lane.lane && tl_lane.generation == generation_ && inited_) return *tl_lane.lane;
+  if (!inited_) init();
+  std::lock_guard<std::mutex> g(mu_);
+  Lane* l = nullptr;
+  for (Lane* c : lanes_)
+    if (!c->in_use && c->generation == generation_) {
+      l = c;
+      break;
+    }
+  if (!l) {
+    l = create_lane_locked();
+    lanes_.push_back(l);
+  }
+  l->in_use = true;
+  tl_lane.lane = l;
+  tl_lane.generation = generation_;
+  return *l;
+}
+
+void Runtime::release_lane(Lane* l, unsigned generation)
+{
+  if (!inited_ || generation != generation_) return;
+  if (l->stream) cudaStreamSynchronize(l->stream);
+  std::lock_guard<std::mutex> g(mu_);
+  l->in_use = false;
+}
+
 void Runtime::finalize()
 {
   std::lock_guard<std::mutex> g(mu_);
   if (!inited_) return;
-  cudaStreamSynchronize(stream_);
-  for (auto& kv : free_blocks_) cudaFree(kv.second);
-  free_blocks_.clear();
+  for (Lane* l : lanes_) {
+    free_lane_locked(l);
+    delete l;
+  }
+  lanes_.clear();
   for (auto& kv : live_blocks_) cudaFree(kv.first);
   live_blocks_.clear();
-  if (scratch_) cudaFree(scratch_);
-  scratch_ = nullptr;
-  scratch_bytes_ = 0;
-  if (counters_) cudaFree(counters_);
-  counters_ = nullptr;
-  if (mbox_h_) cudaFreeHost(mbox_h_);
-  mbox_h_ = mbox_d_ = nullptr;
-  cudaStreamDestroy(stream_);
-  stream_ = nullptr;
+  generation_++;  // lanes still referenced by threads are stale from now on
   inited_ = false;
 }
 
@@ -81,22 +140,24 @@ static size_t round_block(size_t bytes)
 
 void* Runtime::dmalloc(size_t bytes)
 {
-  if (!inited_) init();
+  Lane& L = lane();
   size_t rb = round_block(bytes ? bytes : 1);
   std::lock_guard<std::mutex> g(mu_);
-  auto it = free_blocks_.find(rb);
+  auto it = L.free_blocks.find(rb);
   void* p = nullptr;
-  if (it != free_blocks_.end()) {
+  if (it != L.free_blocks.end()) {
     p = it->second;
-    free_blocks_.erase(it);
+    L.free_blocks.erase(it);
   } else {
     cudaError_t e = cudaMalloc(&p, rb);
     if (e != cudaSuccess) {
-      // release the cache and retry once
+      // release every lane's cache (cudaFree waits for the device) and retry once
       cudaGetLastError();
-      cudaStreamSynchronize(stream_);
-      for (auto& kv : free_blocks_) cudaFree(kv.second);
-      free_blocks_.clear();
+      for (Lane* l : lanes_) {
+        if (l->stream) cudaStreamSynchronize(l->stream);
+        for (auto& kv : l->free_blocks) cudaFree(kv.second);
+        l->free_blocks.clear();
+      }
       e = cudaMalloc(&p, rb);
       if (e != cudaSuccess) {
         cudaGetLastError();
@@ -110,11 +171,12 @@ void* Runtime::dmalloc(size_t bytes)
 
 void Runtime::dfree(void* p)
 {
-  if (!p) return;
+  if (!p || !inited_) return;
+  Lane& L = lane();
   std::lock_guard<std::mutex> g(mu_);
   auto it = live_blocks_.find(p);
   if (it == live_blocks_.end()) return;
-  free_blocks_.emplace(it->second, p);
+  L.free_blocks.emplace(it->second, p);
   live_blocks_.erase(it);
 }
 
@@ -133,9 +195,10 @@ void Runtime::hfree_pinned(void* p)
 
 void Runtime::sync()
 {
-  PB_CUDA(cudaStreamSynchronize(stream_));
-  volatile int* err = (volatile int*)((char*)mbox_h_ + kMailboxResultBytes);
-  if (mbox_h_ && *err != 0) {
+  Lane& L = lane();
+  PB_CUDA(cudaStreamSynchronize(L.stream));
+  volatile int* err = (volatile int*)((char*)L.mbox_h + kMailboxResultBytes);
+  if (*err != 0) {
     const int e = *err;
     *err = 0;
     PB_THROW(PB_FUNCTIONAL_ERROR, "a device-side wait timed out (code %d); results of the last calls are invalid", e);
@@ -144,23 +207,21 @@ void Runtime::sync()
 
 void* Runtime::scratch(size_t bytes)
 {
-  if (!inited_) init();
-  if (bytes > scratch_bytes_) {
+  Lane& L = lane();
+  if (bytes > L.scratch_bytes) {
     // grow: the old buffer may still be read by enqueued kernels
-    PB_CUDA(cudaStreamSynchronize(stream_));
-    if (scratch_) PB_CUDA(cudaFree(scratch_));
+    PB_CUDA(cudaStreamSynchronize(L.stream));
+    if (L.scratch) PB_CUDA(cudaFree(L.scratch));
+    L.scratch = nullptr;
+    L.scratch_bytes = 0;
     size_t nb = bytes < (4u << 20) ? (4u << 20) : bytes * 2;
-    PB_CUDA(cudaMalloc(&scratch_, nb));
-    scratch_bytes_ = nb;
+    PB_CUDA(cudaMalloc(&L.scratch, nb));
+    L.scratch_bytes = nb;
   }
-  return scratch_;
+  return L.scratch;
 }
 
-unsigned int* Runtime::counters()
-{
-  if (!inited_) init();
-  return counters_;
-}
+unsigned int* Runtime::counters() { return lane().counters; }
 
 // ----------------------------------------------------- STREAM benchmarks
 __global__ void k_stream_load(const double* __restrict__ a, int64_t n, double* out)
@@ -474,6 +535,13 @@ void phist_b200_launch_count(uint64_t* count, int* iflag)
 {
   PB_API_BEGIN(iflag);
   *count = rt().launches;
+  PB_API_END(iflag);
+}
+
+void phist_b200_lane_count(int* nlanes, int* iflag)
+{
+  PB_API_BEGIN(iflag);
+  *nlanes = rt().lanes_created();
   PB_API_END(iflag);
 }
 
