@@ -404,6 +404,8 @@ void phist_b200_synchronize(int* iflag);
  * may be shared).  phist_b200_synchronize drains the calling thread's lane;
  * phist_b200_get_stream returns it.  Number of lanes created so far: */
 void phist_b200_lane_count(int* nlanes, int* iflag);
+/* free and total device memory in bytes (admission control of a server) */
+void phist_b200_device_memory(uint64_t* free_bytes, uint64_t* total_bytes, int* iflag);
 /* number of kernel launches this library has issued since init */
 void phist_b200_launch_count(uint64_t* count, int* iflag);
 /* the CUDA stream all kernels are enqueued on (cudaStream_t) */

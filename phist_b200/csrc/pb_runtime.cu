@@ -545,6 +545,17 @@ void phist_b200_lane_count(int* nlanes, int* iflag)
   PB_API_END(iflag);
 }
 
+void phist_b200_device_memory(uint64_t* free_bytes, uint64_t* total_bytes, int* iflag)
+{
+  PB_API_BEGIN(iflag);
+  if (!rt().initialized()) rt().init();
+  size_t f = 0, t = 0;
+  PB_CUDA(cudaMemGetInfo(&f, &t));
+  if (free_bytes) *free_bytes = f;
+  if (total_bytes) *total_bytes = t;
+  PB_API_END(iflag);
+}
+
 void phist_b200_get_stream(void** s, int* iflag)
 {
   PB_API_BEGIN(iflag);

@@ -21,5 +21,7 @@
 #define PHIST_BUILTIN_MEMALIGN 64
 #define PHIST_KERNEL_LIB_B200
 #define PHIST_MVECS_ROW_MAJOR
-#define PHIST_TIMEMONITOR
+/* PHIST_TIMEMONITOR is left undefined: its timer registry is one
+ * process-wide map, and the served form drives PHIST's solvers from several
+ * host threads at once. */
 #endif
