@@ -14,6 +14,8 @@
 // The matrix is stored once more in colour order (CRS), so the rows of one
 // launch are contiguous and their entries are read with coalesced loads.
 #pragma once
+#include <algorithm>
+
 #include "pb_core.hpp"
 
 namespace pb {
@@ -50,70 +52,6 @@ struct KaczArgs {
   T* xr; int64_t ldxr;
   T* xi; int64_t ldxi;       // rc variant only
 };
-
-// one thread per row, NV columns masked to nvec
-template <class T, int NV, bool RC>
-__global__ void __launch_bounds__(256) k_kacz_color(KaczArgs<T> a)
-{
-  const int64_t q = a.q0 + blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
-  if (q >= a.q1) return;
-  const int64_t i = a.rows[q];
-  const int64_t p0 = a.rp[q], p1 = a.rp[q + 1];
-  T tr[NV], ti[NV];
-#pragma unroll
-  for (int j = 0; j < NV; j++) {
-    tr[j] = T(0);
-    ti[j] = T(0);
-    if (j < a.nvec) {
-      const T xr = a.xr[i * a.ldxr + j];
-      if (RC) {
-        const T xi = a.xi[i * a.ldxi + j];
-        tr[j] = -a.sig_r[j] * xr + a.sig_i[j] * xi;
-        ti[j] = -a.sig_i[j] * xr - a.sig_r[j] * xi;
-      } else {
-        tr[j] = -a.sig_r[j] * xr;
-      }
-    }
-  }
-  for (int64_t p = p0; p < p1; p++) {
-    const T v = a.val[p];
-    const int64_t c = a.col[p];
-#pragma unroll
-    for (int j = 0; j < NV; j++)
-      if (j < a.nvec) {
-        tr[j] += v * a.xr[c * a.ldxr + j];
-        if (RC) ti[j] += v * a.xi[c * a.ldxi + j];
-      }
-  }
-  const T nrm = a.nrm[q], d = a.diag[q];
-#pragma unroll
-  for (int j = 0; j < NV; j++)
-    if (j < a.nvec) {
-      if (a.b) tr[j] -= a.b[i * a.ldb + j];
-      T rn = nrm - T(2) * d * a.sig_r[j] + a.sig_r[j] * a.sig_r[j];
-      if (RC) rn += a.sig_i[j] * a.sig_i[j];
-      if (rn == T(0)) rn = T(1);
-      const T f = a.omega[j] / rn;
-      tr[j] *= f;
-      if (RC) {
-        ti[j] *= f;
-        a.xr[i * a.ldxr + j] += tr[j] * a.sig_r[j] + ti[j] * a.sig_i[j];
-        a.xi[i * a.ldxi + j] += ti[j] * a.sig_r[j] - tr[j] * a.sig_i[j];
-      } else {
-        a.xr[i * a.ldxr + j] += tr[j] * a.sig_r[j];
-      }
-    }
-  for (int64_t p = p0; p < p1; p++) {
-    const T v = a.val[p];
-    const int64_t c = a.col[p];
-#pragma unroll
-    for (int j = 0; j < NV; j++)
-      if (j < a.nvec) {
-        a.xr[c * a.ldxr + j] -= tr[j] * v;
-        if (RC) a.xi[c * a.ldxi + j] -= ti[j] * v;
-      }
-  }
-}
 
 // One thread per (row, column): TPR consecutive threads (TPR >= nvec, a power
 // of two) share a row, thread j owns column j.  Within a colour class the
@@ -171,25 +109,22 @@ __global__ void __launch_bounds__(256) k_kacz_color_cols(KaczArgs<T> a)
   }
 }
 
-// Greedy distance-2 colouring in natural row order: row i takes the smallest
-// colour not used by any row that shares a column with it.  colT is the
-// column -> rows pattern (transpose).
-inline int dist2_color(int64_t n, int64_t ncols, const std::vector<int64_t>& rp,
-                       const std::vector<int32_t>& col, std::vector<int32_t>& color)
+// Distance-2 colouring: row i takes the smallest colour not used by any row
+// that shares a column with it (greedy in a given row order), first in
+// natural order, then a few rounds of iterated greedy (rows visited colour
+// class by colour class, classes in reverse order; such a pass never needs
+// more colours than the colouring it starts from, and often fewer).  Fewer
+// colours mean fewer sweep launches and fewer passes over the vector block.
+// colT is the column -> rows pattern (transpose).
+inline int dist2_greedy(int64_t n, const std::vector<int64_t>& rp, const std::vector<int32_t>& col,
+                        const std::vector<int64_t>& tp, const std::vector<int32_t>& trow,
+                        const std::vector<int32_t>& order, std::vector<int32_t>& color)
 {
-  std::vector<int64_t> tp(ncols + 1, 0);
-  for (int64_t p = 0; p < rp[n]; p++) tp[col[p] + 1]++;
-  for (int64_t j = 0; j < ncols; j++) tp[j + 1] += tp[j];
-  std::vector<int32_t> trow(rp[n]);
-  {
-    std::vector<int64_t> fill(tp.begin(), tp.end() - 1);
-    for (int64_t i = 0; i < n; i++)
-      for (int64_t p = rp[i]; p < rp[i + 1]; p++) trow[fill[col[p]]++] = (int32_t)i;
-  }
   color.assign(n, -1);
   std::vector<int64_t> mark;  // mark[c] == i: colour c forbidden for row i
   int ncolor = 0;
-  for (int64_t i = 0; i < n; i++) {
+  for (int64_t k = 0; k < n; k++) {
+    const int64_t i = order.empty() ? k : order[k];
     for (int64_t p = rp[i]; p < rp[i + 1]; p++) {
       const int32_t c = col[p];
       for (int64_t t = tp[c]; t < tp[c + 1]; t++) {
@@ -205,6 +140,45 @@ inline int dist2_color(int64_t n, int64_t ncols, const std::vector<int64_t>& rp,
     while (c < (int)mark.size() && mark[c] == i) c++;
     color[i] = c;
     if (c + 1 > ncolor) ncolor = c + 1;
+  }
+  return ncolor;
+}
+
+inline int dist2_color(int64_t n, int64_t ncols, const std::vector<int64_t>& rp,
+                       const std::vector<int32_t>& col, std::vector<int32_t>& color, int rounds = 8)
+{
+  std::vector<int64_t> tp(ncols + 1, 0);
+  for (int64_t p = 0; p < rp[n]; p++) tp[col[p] + 1]++;
+  for (int64_t j = 0; j < ncols; j++) tp[j + 1] += tp[j];
+  std::vector<int32_t> trow(rp[n]);
+  {
+    std::vector<int64_t> fill(tp.begin(), tp.end() - 1);
+    for (int64_t i = 0; i < n; i++)
+      for (int64_t p = rp[i]; p < rp[i + 1]; p++) trow[fill[col[p]]++] = (int32_t)i;
+  }
+  int ncolor = dist2_greedy(n, rp, col, tp, trow, std::vector<int32_t>(), color);
+  std::vector<int32_t> cur(color), order(n), cand;
+  int ncur = ncolor;
+  for (int r = 0; r < rounds && ncur > 1; r++) {
+    // visit the rows class by class (ascending inside a class): even rounds
+    // in reverse class order, odd rounds largest class first
+    std::vector<int64_t> size(ncur, 0);
+    for (int64_t i = 0; i < n; i++) size[cur[i]]++;
+    std::vector<int> cls(ncur);
+    for (int c = 0; c < ncur; c++) cls[c] = ncur - 1 - c;
+    if (r % 2) std::stable_sort(cls.begin(), cls.end(), [&](int a, int b) { return size[a] > size[b]; });
+    std::vector<int> rank(ncur);
+    for (int k = 0; k < ncur; k++) rank[cls[k]] = k;
+    std::vector<int64_t> start(ncur + 1, 0);
+    for (int64_t i = 0; i < n; i++) start[rank[cur[i]] + 1]++;
+    for (int c = 0; c < ncur; c++) start[c + 1] += start[c];
+    for (int64_t i = 0; i < n; i++) order[start[rank[cur[i]]]++] = (int32_t)i;
+    ncur = dist2_greedy(n, rp, col, tp, trow, order, cand);
+    cur.swap(cand);
+    if (ncur < ncolor) {
+      ncolor = ncur;
+      color = cur;
+    }
   }
   return ncolor;
 }
