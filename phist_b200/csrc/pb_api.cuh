@@ -1100,9 +1100,90 @@ void mvsd_async(RowGemmArgs<T>& a, int BM, int BK)
   }
 }
 
+// fused V*C + Gram on the tensor cores (FP64, widths 8..64 in steps of 8)
+template <int BM, int BK, int MV, int GM>
+bool mvsd_gram_dmma_launch(RowGemmArgs<double>& a)
+{
+  constexpr int R = (BK >= 32 || MV >= 32) ? 64 : 128;
+  constexpr int AP = BM + 4, CP = BK + 4, PT = BK + 4, PVG = MV + 4;
+  constexpr int CSZ = (BM * CP * 8 + 127) / 128 * 128 / 8;
+  constexpr int VSZ = (GM == GM_VW) ? R * PVG : 0;
+  constexpr size_t BYTES3 = 8 * ((size_t)CSZ + 3 * (size_t)R * AP + 3 * (size_t)VSZ + (size_t)R * PT) + 24;
+  constexpr int S = BYTES3 <= 200 * 1024 ? 3 : 2;
+  const double* A = (a.mode == RM_MVSDI) ? (const double*)a.W : a.V;
+  const int64_t lda = (a.mode == RM_MVSDI) ? a.ldw : a.ldv;
+  CUtensorMap mA, mV;
+  if (!make_rows_tmap<double>(&mA, A, a.n, a.m, lda, AP, R)) return false;
+  if (GM == GM_VW) {
+    if (!make_rows_tmap<double>(&mV, a.Vg, a.n, a.mv, a.ldvg, PVG, R)) return false;
+  } else {
+    mV = mA;
+  }
+  const size_t smem = 8 * ((size_t)CSZ + (size_t)S * R * AP + (size_t)S * VSZ + (size_t)R * PT) + 8 * S;
+  const int grid = (int)std::min<int64_t>(ceil_div(a.n, R), (int64_t)rt().num_sms() * 2);
+  const int gm = (GM == GM_WW) ? a.k : a.mv;
+  const int nout = gm * a.k;
+  a.part = (double*)rt().scratch(sizeof(double) * (size_t)grid * nout);
+  a.counter = rt().counters();
+  const bool ext = nout >= 64 && grid > 1;
+  a.R = ext ? -1 : R;
+  auto kern = k_mvsd_gram_dmma<BM, BK, MV, R, S, GM>;
+  set_smem(kern, smem);
+  kern<<<grid, BLK_BS, smem, stream()>>>(a, mA, mV, rt().device_error_word());
+  PB_LAUNCH_CHECK();
+  if (ext) {
+    k_reduce_partials<double><<<(nout + 31) / 32, 256, 0, stream()>>>(a.part, grid, nout, a.Gd, gm, a.ldg, a.galpha,
+                                                                      a.gbeta);
+    PB_LAUNCH_CHECK();
+  }
+  return true;
+}
+
+template <int BM, int BK, int GM>
+bool mvsd_gram_dmma_mv(RowGemmArgs<double>& a, int MV)
+{
+  switch (MV) {
+    case 8: return mvsd_gram_dmma_launch<BM, BK, 8, GM>(a);
+    case 16: return mvsd_gram_dmma_launch<BM, BK, 16, GM>(a);
+    case 32: return mvsd_gram_dmma_launch<BM, BK, 32, GM>(a);
+    default: return mvsd_gram_dmma_launch<BM, BK, 64, GM>(a);
+  }
+}
+
+// true if the fused tensor-core kernel took the product
+inline bool mvsd_gram_dmma(RowGemmArgs<double>& a)
+{
+  if (!rt().use_tma || !rt().use_dmma || a.mode == RM_VCWD || a.gram == GM_NONE) return false;
+  if (a.m > 64 || a.k > 64 || a.m < 5 || a.k < 5) return false;  // widths <= 4: register kernel
+  const int BM = pad_width5(a.m), BK = pad_width5(a.k);
+  if (a.gram == GM_WW) {
+    switch (BM * 100 + BK) {
+#define PB_GW(bm, bk) \
+  case bm * 100 + bk: return mvsd_gram_dmma_launch<bm, bk, bk, GM_WW>(a);
+      PB_GW(8, 8) PB_GW(8, 16) PB_GW(8, 32) PB_GW(8, 64) PB_GW(16, 8) PB_GW(16, 16) PB_GW(16, 32) PB_GW(16, 64)
+      PB_GW(32, 8) PB_GW(32, 16) PB_GW(32, 32) PB_GW(32, 64) PB_GW(64, 8) PB_GW(64, 16) PB_GW(64, 32)
+      PB_GW(64, 64)
+#undef PB_GW
+      default: return false;
+    }
+  }
+  // V'W with the in-place product: square blocks only (BM == BK)
+  if (a.mv < 5 || a.mv > 64 || BM != BK) return false;
+  const int MV = pad_width5(a.mv);
+  switch (BM) {
+    case 8: return mvsd_gram_dmma_mv<8, 8, GM_VW>(a, MV);
+    case 16: return mvsd_gram_dmma_mv<16, 16, GM_VW>(a, MV);
+    case 32: return mvsd_gram_dmma_mv<32, 32, GM_VW>(a, MV);
+    default: return mvsd_gram_dmma_mv<64, 64, GM_VW>(a, MV);
+  }
+}
+inline bool mvsd_gram_dmma(RowGemmArgs<float>&) { return false; }
+
 template <class T>
 void launch_rowgemm(RowGemmArgs<T>& a)
 {
+  // fused V*C + Gram in one pass on the tensor cores
+  if (mvsd_gram_dmma(a)) return;
   {
     // gram-free V*C and in-place W*C on aligned widths: multi-stage staged tiles
     const T* A = (a.mode == RM_MVSDI) ? (const T*)a.W : a.V;

@@ -131,7 +131,8 @@ def test_VC_add_WD(session, oracle, m, k):
         o.delete()
 
 
-@pytest.mark.parametrize("m,k", [(1, 1), (4, 4), (8, 8), (40, 4), (16, 16), (32, 32), (6, 9)])
+@pytest.mark.parametrize("m,k", [(1, 1), (4, 4), (8, 8), (40, 4), (16, 16), (32, 32), (6, 9), (64, 64), (24, 40),
+                                 (64, 8)])
 def test_fused_mvsd_mvTmv(session, oracle, m, k):
     from phist_b200 import kernels as K
     from phist_b200.objects import SdMat
@@ -152,7 +153,8 @@ def test_fused_mvsd_mvTmv(session, oracle, m, k):
         o.delete()
 
 
-@pytest.mark.parametrize("mv,m,k", [(1, 1, 1), (4, 4, 4), (40, 8, 8), (8, 8, 5), (32, 32, 32), (20, 16, 16)])
+@pytest.mark.parametrize("mv,m,k", [(1, 1, 1), (4, 4, 4), (40, 8, 8), (8, 8, 5), (32, 32, 32), (20, 16, 16),
+                                    (64, 64, 64), (12, 24, 24), (64, 16, 13)])
 def test_fused_mvsdi_mvTmv(session, oracle, mv, m, k):
     from phist_b200 import kernels as K
     from phist_b200.objects import SdMat
