@@ -136,6 +136,61 @@ k_coldot(const T* __restrict__ v, int64_t ldv, const T* __restrict__ w, int64_t 
   last_block_reduce<T>(part, NV, gridDim.x, counter, out, 1, NV, 0, T(1), T(0));
 }
 
+// Column dots of two contiguous blocks (ld == nvec, nvec a power of two up
+// to 64, 16-byte aligned) read as flat arrays with 16-byte vector loads:
+// thread t owns the element pair starting at 2t of every chunk of
+// 512*gridDim.x elements, i.e. always the same columns c = 2t mod nvec (and
+// c + 1), so each thread keeps two partial sums.  Four chunks are loaded
+// before they are consumed.  The block sum of column q adds the threads that
+// own q in thread order; the cross-block sum is the usual fixed-order pass.
+template <class T>
+__global__ void __launch_bounds__(256)
+k_coldot_flat(const T* __restrict__ v, const T* __restrict__ w, int64_t total, int nvec, T* part,
+              unsigned int* counter, T* out, int ext)
+{
+  static_assert(sizeof(T) == 8, "double only");
+  __shared__ T red[256][2];
+  const int tid = threadIdx.x;
+  const int64_t stride = (int64_t)gridDim.x * 512;
+  T s0 = T(0), s1 = T(0);
+  int64_t e = (int64_t)blockIdx.x * 512 + 2 * tid;
+  for (; e + 3 * stride + 1 < total; e += 4 * stride) {
+    double2 a[4], b[4];
+#pragma unroll
+    for (int u = 0; u < 4; u++) {
+      a[u] = __ldg(reinterpret_cast<const double2*>(v + e + u * stride));
+      b[u] = __ldg(reinterpret_cast<const double2*>(w + e + u * stride));
+    }
+#pragma unroll
+    for (int u = 0; u < 4; u++) {
+      s0 += a[u].x * b[u].x;
+      s1 += a[u].y * b[u].y;
+    }
+  }
+  for (; e + 1 < total; e += stride) {
+    const double2 a = __ldg(reinterpret_cast<const double2*>(v + e));
+    const double2 b = __ldg(reinterpret_cast<const double2*>(w + e));
+    s0 += a.x * b.x;
+    s1 += a.y * b.y;
+  }
+  if (e < total) s0 += v[e] * w[e];  // odd total (nvec == 1 only)
+  red[tid][0] = s0;
+  red[tid][1] = s1;
+  __syncthreads();
+  if (tid < nvec) {
+    T t = T(0);
+    if (nvec == 1) {
+      for (int k = 0; k < 256; k++) t += red[k][0] + red[k][1];
+    } else {
+      const int half = nvec / 2, q2 = tid / 2, comp = tid & 1;
+      for (int k = q2; k < 256; k += half) t += red[k][comp];
+    }
+    part[(int64_t)blockIdx.x * nvec + tid] = t;
+  }
+  if (ext) return;  // second pass: k_reduce_partials
+  last_block_reduce<T>(part, nvec, gridDim.x, counter, out, 1, nvec, 0, T(1), T(0));
+}
+
 // compensated column dots (PHIST_ROBUST_REDUCTIONS): Dot2 of Ogita, Rump and
 // Oishi per thread, partial (sum, error) pairs combined with TwoSum in a fixed
 // order.  out[2*j] = high part, out[2*j+1] = low part.

@@ -100,6 +100,118 @@ __global__ void k_refine_add(double* x, const TI* __restrict__ d, const double* 
   PB_FOR_ELEMS(n, w, i, j) if (mask[j]) x[i * w + j] += scale[j] * (double)d[i * w + j];
 }
 
+// Fused CG updates on contiguous n x w blocks viewed as flat arrays of
+// N = n*w entries, w a power of two dividing 256: thread t of every block
+// always touches column t mod w (the grid stride is a multiple of w), and
+// the column sums of the fused dot are formed in thread order, then across
+// blocks in block order (last_block_reduce): bitwise reproducible.
+template <class T>
+__device__ __forceinline__ void col_block_sum(T acc, int w, T* part, unsigned int* counter, T* out)
+{
+  __shared__ T red[256];
+  red[threadIdx.x] = acc;
+  __syncthreads();
+  if ((int)threadIdx.x < w) {
+    T s = T(0);
+    for (int k = threadIdx.x; k < 256; k += w) s += red[k];
+    part[(int64_t)blockIdx.x * w + threadIdx.x] = s;
+  }
+  last_block_reduce<T>(part, w, gridDim.x, counter, out, 1, w, 0, T(1), T(0));
+}
+
+// q = p - q and pq_j = p_j' q_j
+template <class T>
+__global__ void __launch_bounds__(256) k_cg_pmq_dot(T* q, const T* __restrict__ p, int64_t N, int w, T* part,
+                                                    unsigned int* counter, T* out)
+{
+  T acc = T(0);
+  const int64_t st = (int64_t)gridDim.x * 256;
+  int64_t e = blockIdx.x * 256 + threadIdx.x;
+  for (; e + 3 * st < N; e += 4 * st) {  // four entries in flight per thread
+    T pv[4], qv[4];
+#pragma unroll
+    for (int u = 0; u < 4; u++) {
+      pv[u] = p[e + u * st];
+      qv[u] = q[e + u * st];
+    }
+#pragma unroll
+    for (int u = 0; u < 4; u++) {
+      qv[u] = pv[u] - qv[u];
+      q[e + u * st] = qv[u];
+      acc += pv[u] * qv[u];
+    }
+  }
+  for (; e < N; e += st) {
+    const T pv = p[e];
+    const T qv = pv - q[e];
+    q[e] = qv;
+    acc += pv * qv;
+  }
+  col_block_sum<T>(acc, w, part, counter, out);
+}
+
+// d += alpha p, r -= alpha q, rr_j = r_j' r_j
+template <class T>
+__global__ void __launch_bounds__(256) k_cg_xr_dot(T* d, T* r, const T* __restrict__ p, const T* __restrict__ q,
+                                                   const T* __restrict__ alpha, int64_t N, int w, T* part,
+                                                   unsigned int* counter, T* out)
+{
+  const T a = alpha[threadIdx.x % w];
+  T acc = T(0);
+  const int64_t st = (int64_t)gridDim.x * 256;
+  int64_t e = blockIdx.x * 256 + threadIdx.x;
+  if (a != T(0)) {
+    for (; e + 3 * st < N; e += 4 * st) {  // four entries in flight per thread
+      T dv[4], rv[4], pv[4], qv[4];
+#pragma unroll
+      for (int u = 0; u < 4; u++) {
+        dv[u] = d[e + u * st];
+        rv[u] = r[e + u * st];
+        pv[u] = p[e + u * st];
+        qv[u] = q[e + u * st];
+      }
+#pragma unroll
+      for (int u = 0; u < 4; u++) {
+        d[e + u * st] = dv[u] + a * pv[u];
+        rv[u] -= a * qv[u];
+        r[e + u * st] = rv[u];
+        acc += rv[u] * rv[u];
+      }
+    }
+  }
+  for (; e < N; e += st) {
+    T rv = r[e];
+    if (a != T(0)) {
+      d[e] += a * p[e];
+      rv -= a * q[e];
+      r[e] = rv;
+    }
+    acc += rv * rv;
+  }
+  col_block_sum<T>(acc, w, part, counter, out);
+}
+
+// p = r + beta p
+template <class T>
+__global__ void __launch_bounds__(256) k_cg_p_flat(T* p, const T* __restrict__ r, const T* __restrict__ beta,
+                                                   int64_t N, int w)
+{
+  const T b = beta[threadIdx.x % w];
+  const int64_t st = (int64_t)gridDim.x * 256;
+  int64_t e = blockIdx.x * 256 + threadIdx.x;
+  for (; e + 3 * st < N; e += 4 * st) {
+    T rv[4], pv[4];
+#pragma unroll
+    for (int u = 0; u < 4; u++) {
+      rv[u] = r[e + u * st];
+      pv[u] = p[e + u * st];
+    }
+#pragma unroll
+    for (int u = 0; u < 4; u++) p[e + u * st] = rv[u] + b * pv[u];
+  }
+  for (; e < N; e += st) p[e] = r[e] + b * p[e];
+}
+
 // one column of a w-wide block into column s of an nsys-wide block and back
 template <class T>
 __global__ void k_col_copy(T* dst, int64_t ldd, const T* __restrict__ src, int64_t lds, int64_t n)
@@ -215,6 +327,9 @@ int carpcg_batch(const SparseMat<double>* A64, const SparseMat<TI>* Ain, int nsy
   }
   int next = 0, unconverged = 0;
   const int gridw = grid_for((int64_t)nw);
+  // fused flat CG kernels when w divides 256
+  const bool flat = (256 % w) == 0;
+  const int gridf = (int)std::max<int64_t>(1, std::min<int64_t>(ceil_div((int64_t)nw, 256 * 8), rt().num_sms() * 8));
 
   CarpWork<TI>* work = carp_build<TI>(Ain, w, sigI.data(), nullptr);
   struct WorkGuard {
@@ -315,18 +430,33 @@ int carpcg_batch(const SparseMat<double>* A64, const SparseMat<TI>* Ain, int nsy
     // one CGMN iteration on every slot
     PB_CUDA(cudaMemcpyAsync(q.p, p.p, sizeof(TI) * nw, cudaMemcpyDeviceToDevice, stream()));
     sweep(nullptr, &mq);  // q = dkswp(p, 0)
-    k_cg_pmq<TI><<<gridw, 256, 0, stream()>>>(q.p, p.p, n, w);
-    PB_LAUNCH_CHECK();
-    dots_dev<TI>(p.p, q.p, n, w, pq.p);
-    k_cg_alpha<TI><<<1, 32, 0, stream()>>>(rr.p, pq.p, active.p, alpha.p, w);
-    PB_LAUNCH_CHECK();
-    k_cg_xr<TI><<<gridw, 256, 0, stream()>>>(d.p, r.p, p.p, q.p, alpha.p, n, w);
-    PB_LAUNCH_CHECK();
-    dots_dev<TI>(r.p, r.p, n, w, rrn.p);
-    k_cg_beta<TI><<<1, 32, 0, stream()>>>(rrn.p, rr.p, active.p, beta.p, w);
-    PB_LAUNCH_CHECK();
-    k_cg_p<TI><<<gridw, 256, 0, stream()>>>(p.p, r.p, beta.p, n, w);
-    PB_LAUNCH_CHECK();
+    if (flat) {
+      TI* part = (TI*)rt().scratch(sizeof(TI) * (size_t)gridf * w);
+      k_cg_pmq_dot<TI><<<gridf, 256, 0, stream()>>>(q.p, p.p, (int64_t)nw, w, part, rt().counters(), pq.p);
+      PB_LAUNCH_CHECK();
+      k_cg_alpha<TI><<<1, 32, 0, stream()>>>(rr.p, pq.p, active.p, alpha.p, w);
+      PB_LAUNCH_CHECK();
+      k_cg_xr_dot<TI><<<gridf, 256, 0, stream()>>>(d.p, r.p, p.p, q.p, alpha.p, (int64_t)nw, w, part,
+                                                   rt().counters(), rrn.p);
+      PB_LAUNCH_CHECK();
+      k_cg_beta<TI><<<1, 32, 0, stream()>>>(rrn.p, rr.p, active.p, beta.p, w);
+      PB_LAUNCH_CHECK();
+      k_cg_p_flat<TI><<<gridf, 256, 0, stream()>>>(p.p, r.p, beta.p, (int64_t)nw, w);
+      PB_LAUNCH_CHECK();
+    } else {
+      k_cg_pmq<TI><<<gridw, 256, 0, stream()>>>(q.p, p.p, n, w);
+      PB_LAUNCH_CHECK();
+      dots_dev<TI>(p.p, q.p, n, w, pq.p);
+      k_cg_alpha<TI><<<1, 32, 0, stream()>>>(rr.p, pq.p, active.p, alpha.p, w);
+      PB_LAUNCH_CHECK();
+      k_cg_xr<TI><<<gridw, 256, 0, stream()>>>(d.p, r.p, p.p, q.p, alpha.p, n, w);
+      PB_LAUNCH_CHECK();
+      dots_dev<TI>(r.p, r.p, n, w, rrn.p);
+      k_cg_beta<TI><<<1, 32, 0, stream()>>>(rrn.p, rr.p, active.p, beta.p, w);
+      PB_LAUNCH_CHECK();
+      k_cg_p<TI><<<gridw, 256, 0, stream()>>>(p.p, r.p, beta.p, n, w);
+      PB_LAUNCH_CHECK();
+    }
     for (int j = 0; j < w; j++)
       if (sys[j] >= 0) {
         iters[sys[j]]++;
