@@ -142,14 +142,15 @@ k_coldot(const T* __restrict__ v, int64_t ldv, const T* __restrict__ w, int64_t 
 // 512*gridDim.x elements, i.e. always the same columns c = 2t mod nvec (and
 // c + 1), so each thread keeps two partial sums.  Four chunks are loaded
 // before they are consumed.  The block sum of column q adds the threads that
-// own q in thread order; the cross-block sum is the usual fixed-order pass.
+// own q in a fixed tree order; the cross-block sum is the usual fixed-order
+// pass.
 template <class T>
 __global__ void __launch_bounds__(256)
 k_coldot_flat(const T* __restrict__ v, const T* __restrict__ w, int64_t total, int nvec, T* part,
               unsigned int* counter, T* out, int ext)
 {
   static_assert(sizeof(T) == 8, "double only");
-  __shared__ T red[256][2];
+  __shared__ T red[2][256];
   const int tid = threadIdx.x;
   const int64_t stride = (int64_t)gridDim.x * 512;
   T s0 = T(0), s1 = T(0);
@@ -174,18 +175,18 @@ k_coldot_flat(const T* __restrict__ v, const T* __restrict__ w, int64_t total, i
     s1 += a.y * b.y;
   }
   if (e < total) s0 += v[e] * w[e];  // odd total (nvec == 1 only)
-  red[tid][0] = s0;
-  red[tid][1] = s1;
-  __syncthreads();
-  if (tid < nvec) {
-    T t = T(0);
-    if (nvec == 1) {
-      for (int k = 0; k < 256; k++) t += red[k][0] + red[k][1];
-    } else {
-      const int half = nvec / 2, q2 = tid / 2, comp = tid & 1;
-      for (int k = q2; k < 256; k += half) t += red[k][comp];
+  if (nvec == 1) {
+    const T t = block_sum_mod<T>(s0 + s1, 1, red[0]);
+    if (tid == 0) part[blockIdx.x] = t;
+  } else {
+    // threads t and t' own the same columns iff t == t' (mod nvec/2)
+    const int half = nvec / 2;
+    const T t0 = block_sum_mod<T>(s0, half, red[0]);
+    const T t1 = block_sum_mod<T>(s1, half, red[1]);
+    if (tid < half) {
+      part[(int64_t)blockIdx.x * nvec + 2 * tid] = t0;
+      part[(int64_t)blockIdx.x * nvec + 2 * tid + 1] = t1;
     }
-    part[(int64_t)blockIdx.x * nvec + tid] = t;
   }
   if (ext) return;  // second pass: k_reduce_partials
   last_block_reduce<T>(part, nvec, gridDim.x, counter, out, 1, nvec, 0, T(1), T(0));

@@ -103,19 +103,14 @@ __global__ void k_refine_add(double* x, const TI* __restrict__ d, const double* 
 // Fused CG updates on contiguous n x w blocks viewed as flat arrays of
 // N = n*w entries, w a power of two dividing 256: thread t of every block
 // always touches column t mod w (the grid stride is a multiple of w), and
-// the column sums of the fused dot are formed in thread order, then across
+// the column sums of the fused dot are formed in a fixed tree, then across
 // blocks in block order (last_block_reduce): bitwise reproducible.
 template <class T>
 __device__ __forceinline__ void col_block_sum(T acc, int w, T* part, unsigned int* counter, T* out)
 {
   __shared__ T red[256];
-  red[threadIdx.x] = acc;
-  __syncthreads();
-  if ((int)threadIdx.x < w) {
-    T s = T(0);
-    for (int k = threadIdx.x; k < 256; k += w) s += red[k];
-    part[(int64_t)blockIdx.x * w + threadIdx.x] = s;
-  }
+  const T s = block_sum_mod<T>(acc, w, red);
+  if ((int)threadIdx.x < w) part[(int64_t)blockIdx.x * w + threadIdx.x] = s;
   last_block_reduce<T>(part, w, gridDim.x, counter, out, 1, w, 0, T(1), T(0));
 }
 

@@ -28,6 +28,25 @@ struct Acc<float> { typedef float type; };
 // out[(o % out_rows)*out_stride_rows + (o / out_rows)*ld_out].
 // Outputs whose row is >= vrows or whose column is >= vcols are padding and
 // are not written.
+// Sum of v over the threads t == c (mod w) of a 256-thread block, for each
+// residue c < w (w a power of two <= 256), returned to thread c; other threads
+// get an unspecified value.  Fixed order: a butterfly over the lanes of each
+// warp, then the warp (or w-strided) partial sums in ascending order.  red
+// holds 256 entries; the caller syncs before it reuses red.
+template <class T>
+__device__ __forceinline__ T block_sum_mod(T v, int w, T* red)
+{
+  for (int off = 16; off >= w; off >>= 1) v += __shfl_xor_sync(0xffffffffu, v, off);
+  red[threadIdx.x] = v;
+  __syncthreads();
+  T s = T(0);
+  if ((int)threadIdx.x < w) {
+    const int step = w > 32 ? w : 32;
+    for (int k = threadIdx.x; k < 256; k += step) s += red[k];
+  }
+  return s;
+}
+
 template <class T>
 __device__ __forceinline__ bool last_block_reduce(const T* part, int nout, int nblocks,
                                                   unsigned int* counter, T* out,
@@ -70,13 +89,22 @@ __device__ __forceinline__ bool last_block_reduce(const T* part, int nout, int n
       for (; b < nblocks; b += G) s += __ldcg(p + (int64_t)b * nout);
     }
     if (G > 1) {
+      // the G group sums of each output are added in a fixed tree: groups
+      // [P, G) onto [0, G-P) (P the largest power of two <= G), then halves
       __syncthreads();
       if (g < G) red[g * span + oo] = s;
       __syncthreads();
-      if (threadIdx.x < span) {
-        s = T(0);
-        for (int gg = 0; gg < G; gg++) s += red[gg * span + threadIdx.x];
+      int P = 1;
+      while (2 * P <= G) P *= 2;
+      if (P < G) {
+        if (g < G - P) red[g * span + oo] += red[(g + P) * span + oo];
+        __syncthreads();
       }
+      for (int h = P / 2; h >= 1; h >>= 1) {
+        if (g < h) red[g * span + oo] += red[(g + h) * span + oo];
+        __syncthreads();
+      }
+      if (threadIdx.x < span) s = red[threadIdx.x];
     }
     if (threadIdx.x < span) {
       const int o = o0 + threadIdx.x;

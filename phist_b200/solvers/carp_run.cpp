@@ -148,11 +148,12 @@ int main(int argc, char** argv)
   }
 
   std::vector<double> walls, relres(nshifts, 0.0);
-  std::vector<int> refines, conv(nshifts, 0), batch_iters;
+  std::vector<int> refines, fp64_steps, conv(nshifts, 0), batch_iters;
   uint64_t launches = 0;
   for (int rep = 0; rep < reps; rep++) {
     CHK(phist_Dmvec_put_value(X, 0.0, &iflag));
     refines.clear();
+    fp64_steps.clear();
     uint64_t l0 = 0, l1 = 0;
     CHK(phist_b200_launch_count(&l0, &iflag));
     CHK(phist_b200_synchronize(&iflag));
@@ -185,6 +186,9 @@ int main(int argc, char** argv)
           return 1;
         }
         refines.push_back(nref);
+        int s32 = 0, s64 = 0;
+        CHK(phist_b200_mixed_carp_stats(M, &s32, &s64, &iflag));
+        fp64_steps.push_back(s64);
         CHK(phist_b200_mixed_carp_delete(M, &iflag));
       } else {
         phist_Dcarp_cgState_ptr S = NULL;
@@ -230,6 +234,8 @@ int main(int argc, char** argv)
   printf("{\"problem\": \"%s\", \"mixed\": %d, \"innerTol\": %.3e, \"refinements\": [", problem, mixed,
          innerTol);
   for (size_t i = 0; i < refines.size(); i++) printf("%s%d", i ? ", " : "", refines[i]);
+  printf("], \"fp64_refinements\": [");
+  for (size_t i = 0; i < fp64_steps.size(); i++) printf("%s%d", i ? ", " : "", fp64_steps[i]);
   printf("], \"n\": %d, \"nshifts\": %d, \"block\": %d, \"tol\": %.3e, \"maxIter\": %d, "
          "\"omega\": %g, \"nconv\": %d, \"launches\": %llu, \"max_relres\": ",
          nloc, nshifts, block, tol, maxIter, omega, nconv, (unsigned long long)launches);

@@ -84,6 +84,8 @@ def test_carp_cg_mixed_refinement(session, tmp_path):
             "maxIter=40000", "seed=%d" % seed, "mixed=1", "innerTol=1e-5", "out=" + out)
     assert r["mixed"] == 1 and r["nconv"] == ns
     assert all(k >= 2 for k in r["refinements"])
+    # corrections solved in FP64 once FP32 stopped paying: never more than all
+    assert all(0 <= f <= k for f, k in zip(r["fp64_refinements"], r["refinements"]))
     rp, c, v = honeycomb(L, L, seed)
     n = len(rp) - 1
     shifts = 2.5 * unif(seed, np.arange(ns, dtype=np.uint64))
