@@ -395,6 +395,10 @@ void phist_b200_set_spmv_config(int nvec, int tpr, int unroll, int* iflag);
 /* block widths >= min_nvec (8..32) use the SpMMV kernel that stages the
  * gathered X rows in shared memory (values above 32 disable it) */
 void phist_b200_set_spmv_staged(int min_nvec, int* iflag);
+/* batched CARP-CG: replay each iteration as a recorded CUDA graph (1, the
+ * default; environment PHIST_B200_GRAPHS) or launch its kernels one by one
+ * (0); both give bitwise identical results */
+void phist_b200_set_graphs(int on, int* iflag);
 /* wait for all work this library enqueued */
 void phist_b200_synchronize(int* iflag);
 /* Every host thread that calls the library works on its own lane: a CUDA

@@ -245,16 +245,22 @@ void as_mvec(Mvec<T>& m, T* d, int64_t n, int w)
   m.h_base = nullptr;
 }
 
-// column dots a'b of two n x w blocks into a device array out[w]
+// blocks of the column-dot kernel for n rows (the partial sums need
+// dots_grid(n) * 32 entries)
+inline int dots_grid(int64_t n) { return std::max(1, std::min(grid_for(n), rt().num_sms() * 4)); }
+
+// column dots a'b of two n x w blocks into a device array out[w]; part and
+// counter default to the lane's scratch and arrival counter
 template <class T>
-void dots_dev(const T* a, const T* b, int64_t n, int w, T* out)
+void dots_dev(const T* a, const T* b, int64_t n, int w, T* out, T* part = nullptr, unsigned int* counter = nullptr)
 {
-  const int grid = std::max(1, std::min(grid_for(n), rt().num_sms() * 4));
-  T* part = (T*)rt().scratch(sizeof(T) * (size_t)grid * 32);
+  const int grid = dots_grid(n);
+  if (!part) part = (T*)rt().scratch(sizeof(T) * (size_t)grid * 32);
+  if (!counter) counter = rt().counters();
 #define PB_DD(NVv)                                                                                     \
   {                                                                                                    \
     const int ext = (NVv >= 16 && grid > 1) ? 1 : 0;                                                   \
-    k_coldot<T, NVv><<<grid, 256, 0, stream()>>>(a, w, b, w, n, w, part, rt().counters(), out, ext);   \
+    k_coldot<T, NVv><<<grid, 256, 0, stream()>>>(a, w, b, w, n, w, part, counter, out, ext);           \
     if (ext) k_reduce_partials<T><<<1, 256, 0, stream()>>>(part, grid, NVv, out, NVv, 0, T(1), T(0));  \
   }
   if (w <= 1) PB_DD(1)
@@ -331,11 +337,19 @@ int carpcg_batch(const SparseMat<double>* A64, const SparseMat<TI>* Ain, int nsy
     CarpWork<TI>* w;
     ~WorkGuard() { carp_free<TI>(w); }
   } guard{work};
+  // partial sums and arrival counter of the iteration's dots: buffers of
+  // their own, so that the pointers recorded in the CUDA graph stay valid
+  // whatever the lane's scratch does in between
+  DevBuf<TI> ipart((size_t)std::max<int64_t>((int64_t)gridf * w, (int64_t)dots_grid(n) * 32));
+  DevBuf<unsigned int> icnt(1);
+  PB_CUDA(cudaMemsetAsync(icnt.p, 0, sizeof(unsigned int), stream()));
 
   auto sweep = [&](const Mvec<TI>* rhs, Mvec<TI>* v) {
     carp_run<TI, false>(work, w, sigI.data(), nullptr, rhs, v, nullptr, omegaI.data());
   };
+  bool graph_stale = true;  // the shifts recorded in the graph changed
   auto set_shift = [&](int j, double sg) {
+    graph_stale = true;
     sig[j] = sg;
     negsig[j] = -sg;
     sigI[j] = (TI)sg;
@@ -418,21 +432,18 @@ int carpcg_batch(const SparseMat<double>* A64, const SparseMat<TI>* Ain, int nsy
     std::iota(all.begin(), all.end(), 0);
     refill(all);
   }
-  for (int it = 1;; it++) {
-    bool any = false;
-    for (int j = 0; j < w; j++) any = any || sys[j] >= 0;
-    if (!any) break;
-    // one CGMN iteration on every slot
+  // one CGMN iteration on every slot: only kernel launches and a device
+  // copy, all scalars device-resident, so it can be recorded as a graph
+  auto iteration = [&]() {
     PB_CUDA(cudaMemcpyAsync(q.p, p.p, sizeof(TI) * nw, cudaMemcpyDeviceToDevice, stream()));
     sweep(nullptr, &mq);  // q = dkswp(p, 0)
     if (flat) {
-      TI* part = (TI*)rt().scratch(sizeof(TI) * (size_t)gridf * w);
-      k_cg_pmq_dot<TI><<<gridf, 256, 0, stream()>>>(q.p, p.p, (int64_t)nw, w, part, rt().counters(), pq.p);
+      k_cg_pmq_dot<TI><<<gridf, 256, 0, stream()>>>(q.p, p.p, (int64_t)nw, w, ipart.p, icnt.p, pq.p);
       PB_LAUNCH_CHECK();
       k_cg_alpha<TI><<<1, 32, 0, stream()>>>(rr.p, pq.p, active.p, alpha.p, w);
       PB_LAUNCH_CHECK();
-      k_cg_xr_dot<TI><<<gridf, 256, 0, stream()>>>(d.p, r.p, p.p, q.p, alpha.p, (int64_t)nw, w, part,
-                                                   rt().counters(), rrn.p);
+      k_cg_xr_dot<TI><<<gridf, 256, 0, stream()>>>(d.p, r.p, p.p, q.p, alpha.p, (int64_t)nw, w, ipart.p, icnt.p,
+                                                   rrn.p);
       PB_LAUNCH_CHECK();
       k_cg_beta<TI><<<1, 32, 0, stream()>>>(rrn.p, rr.p, active.p, beta.p, w);
       PB_LAUNCH_CHECK();
@@ -441,23 +452,73 @@ int carpcg_batch(const SparseMat<double>* A64, const SparseMat<TI>* Ain, int nsy
     } else {
       k_cg_pmq<TI><<<gridw, 256, 0, stream()>>>(q.p, p.p, n, w);
       PB_LAUNCH_CHECK();
-      dots_dev<TI>(p.p, q.p, n, w, pq.p);
+      dots_dev<TI>(p.p, q.p, n, w, pq.p, ipart.p, icnt.p);
       k_cg_alpha<TI><<<1, 32, 0, stream()>>>(rr.p, pq.p, active.p, alpha.p, w);
       PB_LAUNCH_CHECK();
       k_cg_xr<TI><<<gridw, 256, 0, stream()>>>(d.p, r.p, p.p, q.p, alpha.p, n, w);
       PB_LAUNCH_CHECK();
-      dots_dev<TI>(r.p, r.p, n, w, rrn.p);
+      dots_dev<TI>(r.p, r.p, n, w, rrn.p, ipart.p, icnt.p);
       k_cg_beta<TI><<<1, 32, 0, stream()>>>(rrn.p, rr.p, active.p, beta.p, w);
       PB_LAUNCH_CHECK();
       k_cg_p<TI><<<gridw, 256, 0, stream()>>>(p.p, r.p, beta.p, n, w);
       PB_LAUNCH_CHECK();
     }
+  };
+  // The iteration as a CUDA graph, replayed K times between two checks: one
+  // graph launch instead of ~2 ncolors + 5 kernel launches per iteration.
+  // The shifts are kernel arguments, so a refill that changes them records
+  // the graph again.
+  struct GraphGuard {
+    cudaGraphExec_t g = nullptr;
+    ~GraphGuard()
+    {
+      if (g) cudaGraphExecDestroy(g);
+    }
+  } graph;
+  uint64_t graph_launches = 0;
+  auto record = [&]() {
+    if (graph.g) {
+      PB_CUDA(cudaGraphExecDestroy(graph.g));
+      graph.g = nullptr;
+    }
+    const uint64_t l0 = rt().launches.load();
+    PB_CUDA(cudaStreamBeginCapture(stream(), cudaStreamCaptureModeThreadLocal));
+    cudaGraph_t g = nullptr;
+    try {
+      iteration();
+    } catch (...) {
+      cudaStreamEndCapture(stream(), &g);
+      if (g) cudaGraphDestroy(g);
+      throw;
+    }
+    PB_CUDA(cudaStreamEndCapture(stream(), &g));
+    graph_launches = rt().launches.load() - l0;
+    rt().launches -= graph_launches;  // counted when the graph runs
+    const cudaError_t e = cudaGraphInstantiate(&graph.g, g, 0);
+    cudaGraphDestroy(g);
+    PB_CUDA(e);
+    graph_stale = false;
+  };
+
+  for (;;) {
+    bool any = false;
+    for (int j = 0; j < w; j++) any = any || sys[j] >= 0;
+    if (!any) break;
+    // K CGMN iterations on every slot
+    if (rt().use_graphs) {
+      if (graph_stale || !graph.g) record();
+      for (int k = 0; k < K; k++) {
+        PB_CUDA(cudaGraphLaunch(graph.g, stream()));
+        rt().launches += graph_launches;
+      }
+    } else {
+      for (int k = 0; k < K; k++) iteration();
+    }
     for (int j = 0; j < w; j++)
       if (sys[j] >= 0) {
-        iters[sys[j]]++;
-        inner_it[j]++;
+        iters[sys[j]] += K;
+        inner_it[j] += K;
       }
-    if (it % K != 0) continue;
 
     // ---- check
     std::vector<int> done;  // slots whose system converged or ran out of iterations

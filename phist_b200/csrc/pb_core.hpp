@@ -191,6 +191,8 @@ class Runtime {
   bool use_tma = true;
   // FP64 block products on the tensor cores (DMMA) for widths multiple of 8
   bool use_dmma = true;
+  // batched CARP-CG replays its iteration as a CUDA graph (PHIST_B200_GRAPHS=0: plain launches)
+  bool use_graphs = true;
 
   // statistics: kernel launches issued by this library (all lanes)
   std::atomic<uint64_t> launches{0};

@@ -39,6 +39,7 @@ void Runtime::init()
   if (const char* v = getenv("PHIST_B200_VERBOSE")) verbose = atoi(v);
   if (const char* v = getenv("PHIST_B200_TMA")) use_tma = atoi(v) != 0;
   if (const char* v = getenv("PHIST_B200_DMMA")) use_dmma = atoi(v) != 0;
+  if (const char* v = getenv("PHIST_B200_GRAPHS")) use_graphs = atoi(v) != 0;
   if (const char* c = getenv("PHIST_B200_SELL_C")) sell_C = atoi(c);
   if (const char* s = getenv("PHIST_B200_SELL_SIGMA")) sell_sigma_default = atoll(s);
   inited_ = true;
@@ -521,6 +522,13 @@ void phist_b200_set_spmv_staged(int min_nvec, int* iflag)
 {
   PB_API_BEGIN(iflag);
   rt().spmv_staged_min_nvec = min_nvec;
+  PB_API_END(iflag);
+}
+
+void phist_b200_set_graphs(int on, int* iflag)
+{
+  PB_API_BEGIN(iflag);
+  rt().use_graphs = on != 0;
   PB_API_END(iflag);
 }
 

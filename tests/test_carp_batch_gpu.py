@@ -78,3 +78,21 @@ def test_batch_unconverged_is_reported(session):
 def test_batch_no_systems(session):
     *_, iflag = _run("HONEYCOMB-8-S4-W1", 0, 4, 0)
     assert iflag == 0
+
+
+@pytest.mark.parametrize("mixed", [0, 1])
+def test_batch_graph_replay_is_bitwise_identical(session, mixed):
+    """the iteration replayed as a CUDA graph and launched kernel by kernel
+    give the same iterates bit for bit (refills re-record the graph: 9
+    systems through 4 slots)"""
+    from phist_b200 import kernels as K
+    K.chk(K.phist_b200_set_graphs, 0)
+    try:
+        *_, x0, it0, rel0, f0 = _run("HONEYCOMB-16x12-S2-W1", 9, 4, mixed)
+    finally:
+        K.chk(K.phist_b200_set_graphs, 1)
+    *_, x1, it1, rel1, f1 = _run("HONEYCOMB-16x12-S2-W1", 9, 4, mixed)
+    assert f0 == f1 == 0
+    np.testing.assert_array_equal(it0, it1)
+    np.testing.assert_array_equal(x0, x1)
+    np.testing.assert_array_equal(rel0, rel1)
