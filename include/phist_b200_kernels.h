@@ -399,6 +399,35 @@ void phist_b200_set_spmv_staged(int min_nvec, int* iflag);
  * default; environment PHIST_B200_GRAPHS) or launch its kernels one by one
  * (0); both give bitwise identical results */
 void phist_b200_set_graphs(int on, int* iflag);
+/* kernel-path switches, all on by default (1) and each also read from the
+ * environment at init: "tma" (TMA-staged block products, PHIST_B200_TMA),
+ * "dmma" (FP64 tensor-core tiles, PHIST_B200_DMMA), "graphs" (as
+ * phist_b200_set_graphs, PHIST_B200_GRAPHS).  "graphs" never changes a
+ * result; tma/dmma change the summation order of the block products.
+ * Unknown names: PHIST_INVALID_INPUT. */
+void phist_b200_set_option(const char* name, int value, int* iflag);
+/* SpMMV autotuner (no PHIST counterpart: GHOST fixes C = 32 on CUDA and sigma
+ * by flag, src/kernels/ghost/kernels.cpp:69-134).  Times Y = A X on A itself
+ * for each block width in widths[nw] (1..32) over the SELL layouts C in
+ * {32, 16, 8} x sigma in {1, 4C, 1024} (sigma 1 only if all rows have the
+ * same length) and the SpMMV kernel variants of each width (threads per
+ * row, fully unrolled short-row kernel, shared-memory staged kernel), each
+ * the median of reps device-timed calls after an L2 flush.  A is left in the
+ * layout with the least total time, with the fastest variant per width;
+ * best_us[nw] (may be NULL) receives each width's time there.  Results of
+ * every SpMMV are bitwise the same in every layout and variant; vectors keep
+ * their row order. */
+void phist_b200_DsparseMat_autotune(phist_DsparseMat_ptr A, int nw, const int* widths, int reps,
+                                    double* best_us, int* iflag);
+void phist_b200_SsparseMat_autotune(phist_SsparseMat_ptr A, int nw, const int* widths, int reps,
+                                    double* best_us, int* iflag);
+/* the configuration in effect: SELL chunk height and sorting window, and per
+ * width class 1, 2, 4, 8, 16, 32 (arrays of 6, each may be NULL): threads
+ * per row, unrolled short-row kernel (0/1), staged kernel (0/1) */
+void phist_b200_DsparseMat_get_tuning(phist_Dconst_sparseMat_ptr A, int* C, int64_t* sigma, int* tpr,
+                                      int* unroll, int* staged, int* iflag);
+void phist_b200_SsparseMat_get_tuning(phist_Sconst_sparseMat_ptr A, int* C, int64_t* sigma, int* tpr,
+                                      int* unroll, int* staged, int* iflag);
 /* wait for all work this library enqueued */
 void phist_b200_synchronize(int* iflag);
 /* Every host thread that calls the library works on its own lane: a CUDA

@@ -18,6 +18,7 @@ import ctypes as ct
 import json
 import os
 import sys
+import time
 
 import numpy as np
 
@@ -237,6 +238,54 @@ def suite_latency(T, reps, peak, n=262144):
         out.append(line)
     for o in (X1, Y1, X4, Y4, V, C, C44, A):
         o.delete()
+    return out
+
+
+def suite_autotune(T, reps, peak, L=128):
+    """SpMMV before and after the autotuner (SELL C, sigma and kernel variant
+    per width chosen by timing) on the Anderson L=128 matrix (7 entries in
+    every row) and the Dirichlet Laplacian 128^3 (4 to 7 entries)"""
+    out = []
+    for prob in ("ANDERSON3D-%d-S1" % L, "LAPLACE3D-%d" % L):
+        out += _autotune_one(T, reps, peak, prob)
+    return out
+
+
+def _autotune_one(T, reps, peak, prob):
+    from . import kernels as K
+    from .generators import random_block
+    from .objects import Mvec, SparseMat
+    K.chk(K.phist_b200_set_sell_params, 32, 256)
+    A = SparseMat.from_problem(prob, flags=K.PHIST_SPARSEMAT_PERM_LOCAL)
+    n, nnz = A.nrows, A.nnz
+    widths = [1, 2, 4, 8, 16, 32]
+    out = []
+
+    def sweep(tag):
+        for nv in widths:
+            X = Mvec(A.domain_map, nv).set(random_block(n, nv, 3))
+            Y = Mvec(A.row_map, nv)
+            b = nnz * 12 + 16 * n * nv + (-(-n // 32)) * 12
+            t = T.time(lambda: K.chk(K.phist_DsparseMat_times_mvec, 1.0, A.h, X.h, 0.0, Y.h), reps)
+            out.append(report("spmmv_" + tag, {"problem": prob, "n": n, "nnz": nnz, "nvec": nv}, b, 2 * nnz * nv,
+                              t, peak))
+            X.delete()
+            Y.delete()
+
+    sweep("default")
+    wd = np.array(widths, np.int32)
+    best = np.zeros(len(widths))
+    t0 = time.perf_counter()
+    K.chk(K.phist_b200_DsparseMat_autotune, A.h, len(widths), K.ptr(wd), 5, K.ptr(best))
+    wall = time.perf_counter() - t0
+    C, sig = ct.c_int(), ct.c_int64()
+    tpr, unr, stg = (np.zeros(6, np.int32) for _ in range(3))
+    K.chk(K.phist_b200_DsparseMat_get_tuning, A.h, ct.byref(C), ct.byref(sig), K.ptr(tpr), K.ptr(unr), K.ptr(stg))
+    line = {"autotune": {"problem": prob, "C": C.value, "sigma": sig.value, "tpr": tpr.tolist(), "unroll": unr.tolist(),
+                         "staged": stg.tolist(), "tuner_us": [round(x, 2) for x in best], "wall_s": round(wall, 2)}}
+    print(json.dumps(line), flush=True)
+    sweep("tuned")
+    A.delete()
     return out
 
 

@@ -383,58 +383,41 @@ void* upload_vec(const std::vector<T>& v)
   return d;
 }
 
-// rows stably sorted by column inside each row (the builtin's
-// sort_global_cols, crsmat_module.F90:484-516), then laid out as SELL-C-sigma
+// SELL-C-sigma layout of the CRS rows (columns sorted inside each row):
+// rows stably sorted by descending length inside windows of sigma rows,
+// chunks of C rows padded to the chunk's longest row, entry k of chunk row l
+// at chunk_ptr + k*C + l.  Replaces any layout A had; the result of every
+// SpMMV is the same in every layout (each row sums its entries in column
+// order).
 template <class T>
-SparseMat<T>* build_sparse(const Comm* comm, int64_t nrows, int64_t ncols,
-                           std::vector<int64_t>&& rp, std::vector<int32_t>&& col,
-                           std::vector<T>&& val, int flags)
+void sell_layout(SparseMat<T>* A, const std::vector<int64_t>& rp, const std::vector<int32_t>& col,
+                 const std::vector<T>& val, int C, int64_t sigma)
 {
-  ensure_init();
-  PB_REQUIRE(nrows >= 0 && nrows < (int64_t(1) << 31) && ncols >= 0 && ncols < (int64_t(1) << 31),
-             PB_INTEGER_OVERFLOW, "matrix dimensions %lld x %lld exceed 32-bit local indices",
-             (long long)nrows, (long long)ncols);
-  const int64_t nnz = rp[nrows];
-  // sort columns inside rows (stable)
-  {
-    std::vector<int64_t> idx;
-    std::vector<int32_t> c2;
-    std::vector<T> v2;
-    for (int64_t i = 0; i < nrows; i++) {
-      const int64_t p0 = rp[i], p1 = rp[i + 1], len = p1 - p0;
-      bool sorted = true;
-      for (int64_t p = p0 + 1; p < p1; p++)
-        if (col[p] < col[p - 1]) { sorted = false; break; }
-      if (sorted) continue;
-      idx.resize(len);
-      std::iota(idx.begin(), idx.end(), p0);
-      std::stable_sort(idx.begin(), idx.end(), [&](int64_t a, int64_t b) { return col[a] < col[b]; });
-      c2.resize(len);
-      v2.resize(len);
-      for (int64_t q = 0; q < len; q++) { c2[q] = col[idx[q]]; v2[q] = val[idx[q]]; }
-      for (int64_t q = 0; q < len; q++) { col[p0 + q] = c2[q]; val[p0 + q] = v2[q]; }
-    }
-  }
-  for (int64_t p = 0; p < nnz; p++)
-    PB_REQUIRE(col[p] >= 0 && col[p] < ncols, PB_INVALID_INPUT,
-               "column index %d out of range [0,%lld)", col[p], (long long)ncols);
-
-  SparseMat<T>* A = new SparseMat<T>();
-  A->comm = comm;
-  A->nrows = nrows;
-  A->ncols = ncols;
-  A->nnz = nnz;
-  A->C = rt().sell_C;
-  A->sigma = (flags & (PB_SPARSEMAT_PERM_LOCAL | PB_SPARSEMAT_PERM_GLOBAL)) ? rt().sell_sigma_default : 1;
-  if (A->sigma < 1) A->sigma = 1;
-  const int C = A->C;
+  PB_REQUIRE(C >= 1 && C <= 1024, PB_INVALID_INPUT, "SELL chunk height %d out of range", C);
+  const int64_t nrows = A->nrows;
+  if (sigma < 1) sigma = 1;
+  rt().sync();  // the old layout may still be read by enqueued kernels
+  rt().dfree(A->d_chunk_ptr);
+  rt().dfree(A->d_chunk_len);
+  rt().dfree(A->d_col);
+  rt().dfree(A->d_val);
+  rt().dfree(A->d_perm);
+  rt().dfree(A->d_row_len);
+  A->d_chunk_ptr = nullptr;
+  A->d_chunk_len = nullptr;
+  A->d_col = nullptr;
+  A->d_val = nullptr;
+  A->d_perm = nullptr;
+  A->d_row_len = nullptr;
+  A->C = C;
+  A->sigma = sigma;
 
   // sigma permutation: stable descending row length inside windows
   std::vector<int32_t> perm(nrows);
   std::iota(perm.begin(), perm.end(), 0);
-  if (A->sigma > 1) {
-    for (int64_t w0 = 0; w0 < nrows; w0 += A->sigma) {
-      const int64_t w1 = std::min(nrows, w0 + A->sigma);
+  if (sigma > 1) {
+    for (int64_t w0 = 0; w0 < nrows; w0 += sigma) {
+      const int64_t w1 = std::min(nrows, w0 + sigma);
       std::stable_sort(perm.begin() + w0, perm.begin() + w1, [&](int32_t a, int32_t b) {
         return (rp[a + 1] - rp[a]) > (rp[b + 1] - rp[b]);
       });
@@ -478,18 +461,66 @@ SparseMat<T>* build_sparse(const Comm* comm, int64_t nrows, int64_t ncols,
       }
     }
   }
-  std::vector<T> diag(nrows, T(0));
-  for (int64_t i = 0; i < nrows; i++)
-    for (int64_t p = rp[i]; p < rp[i + 1]; p++)
-      if (col[p] == i) diag[i] = val[p];
-
   A->d_chunk_ptr = (int64_t*)upload_vec(cptr);
   A->d_chunk_len = (int32_t*)upload_vec(clen);
   A->d_col = (int32_t*)upload_vec(scol);
   A->d_val = (T*)upload_vec(sval);
   A->d_perm = ident ? nullptr : (int32_t*)upload_vec(perm);
   A->d_row_len = (int32_t*)upload_vec(rlen);
-  A->d_diag = (T*)upload_vec(diag);
+  A->h_perm = std::move(perm);
+  rt().sync();
+}
+
+// rows stably sorted by column inside each row (the builtin's
+// sort_global_cols, crsmat_module.F90:484-516), then laid out as SELL-C-sigma
+template <class T>
+SparseMat<T>* build_sparse(const Comm* comm, int64_t nrows, int64_t ncols,
+                           std::vector<int64_t>&& rp, std::vector<int32_t>&& col,
+                           std::vector<T>&& val, int flags)
+{
+  ensure_init();
+  PB_REQUIRE(nrows >= 0 && nrows < (int64_t(1) << 31) && ncols >= 0 && ncols < (int64_t(1) << 31),
+             PB_INTEGER_OVERFLOW, "matrix dimensions %lld x %lld exceed 32-bit local indices",
+             (long long)nrows, (long long)ncols);
+  const int64_t nnz = rp[nrows];
+  // sort columns inside rows (stable)
+  {
+    std::vector<int64_t> idx;
+    std::vector<int32_t> c2;
+    std::vector<T> v2;
+    for (int64_t i = 0; i < nrows; i++) {
+      const int64_t p0 = rp[i], p1 = rp[i + 1], len = p1 - p0;
+      bool sorted = true;
+      for (int64_t p = p0 + 1; p < p1; p++)
+        if (col[p] < col[p - 1]) { sorted = false; break; }
+      if (sorted) continue;
+      idx.resize(len);
+      std::iota(idx.begin(), idx.end(), p0);
+      std::stable_sort(idx.begin(), idx.end(), [&](int64_t a, int64_t b) { return col[a] < col[b]; });
+      c2.resize(len);
+      v2.resize(len);
+      for (int64_t q = 0; q < len; q++) { c2[q] = col[idx[q]]; v2[q] = val[idx[q]]; }
+      for (int64_t q = 0; q < len; q++) { col[p0 + q] = c2[q]; val[p0 + q] = v2[q]; }
+    }
+  }
+  for (int64_t p = 0; p < nnz; p++)
+    PB_REQUIRE(col[p] >= 0 && col[p] < ncols, PB_INVALID_INPUT,
+               "column index %d out of range [0,%lld)", col[p], (long long)ncols);
+
+  SparseMat<T>* A = new SparseMat<T>();
+  A->comm = comm;
+  A->nrows = nrows;
+  A->ncols = ncols;
+  A->nnz = nnz;
+  const int64_t sigma = (flags & (PB_SPARSEMAT_PERM_LOCAL | PB_SPARSEMAT_PERM_GLOBAL)) ? rt().sell_sigma_default : 1;
+  sell_layout(A, rp, col, val, rt().sell_C, sigma);
+  {
+    std::vector<T> diag(nrows, T(0));
+    for (int64_t i = 0; i < nrows; i++)
+      for (int64_t p = rp[i]; p < rp[i + 1]; p++)
+        if (col[p] == i) diag[i] = val[p];
+    A->d_diag = (T*)upload_vec(diag);
+  }
   rt().sync();
 
   A->row_map = new Map();
@@ -512,7 +543,6 @@ SparseMat<T>* build_sparse(const Comm* comm, int64_t nrows, int64_t ncols,
   A->h_row_ptr = std::move(rp);
   A->h_col = std::move(col);
   A->h_val = std::move(val);
-  A->h_perm = std::move(perm);
   // the uploads ran on the creating thread's lane: drain it, so that the
   // (read-only) matrix can be used from any thread's lane right away
   rt().sync();
@@ -655,11 +685,14 @@ void launch_spmv_nv(const SparseMat<T>* A, const SellDev<T>& S, SpmvArgs<T>& p, 
     p.part = (T*)rt().scratch(sizeof(T) * (size_t)grid * 2 * NV);
     p.counter = rt().counters();
   }
-  const bool fast = rt().spmv_unroll && A->C == 32 && A->max_row_len <= 8;
+  constexpr int LG = NV == 1 ? 0 : NV == 2 ? 1 : NV == 4 ? 2 : NV == 8 ? 3 : NV == 16 ? 4 : 5;
+  const bool unroll = A->tune_unroll[LG] >= 0 ? A->tune_unroll[LG] != 0 : rt().spmv_unroll;
+  const bool fast = unroll && A->C == 32 && A->max_row_len <= 8;
   const bool dots = p.want_wdw || p.want_vdw;
   if constexpr (NV >= 8 && NV <= 32) {
     // wide block vectors: X rows staged in shared memory by cp.async
-    if (fast && vec && !dots && !p.u && NV >= rt().spmv_staged_min_nvec) {
+    const bool staged = A->tune_staged[LG] >= 0 ? A->tune_staged[LG] != 0 : NV >= rt().spmv_staged_min_nvec;
+    if (fast && vec && !dots && !p.u && staged) {
       const size_t smem = StagedSmem<T, NV>::bytes;
       const int bps = std::max(1, std::min(8, (int)((200 * 1024) / smem)));
       const int sgrid = (int)std::min<int64_t>(A->nchunks > 0 ? A->nchunks : 1, (int64_t)rt().num_sms() * bps);
@@ -707,7 +740,7 @@ void spmv_tile(const SparseMat<T>* A, SpmvArgs<T>& p, int nv)
           (p.ldy % vw == 0) && (!p.u || (aligned16<T>(p.u + p.col0) && p.ldu % vw == 0));
     if (sizeof(T) == 4 && NV == 2) vec = false;
   }
-  const int tpr = rt().spmv_tpr[lg];
+  const int tpr = A->tune_tpr[lg] > 0 ? A->tune_tpr[lg] : rt().spmv_tpr[lg];
   switch (NV) {
     case 1: launch_spmv_nv<T, 1, 1>(A, S, p, false); break;
     case 2: launch_spmv_nv<T, 2, 1>(A, S, p, vec); break;

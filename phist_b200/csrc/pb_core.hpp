@@ -142,6 +142,7 @@ class Runtime {
   cudaStream_t stream() { return lane().stream; }
   int device() const { return device_; }
   int num_sms() const { return num_sms_; }
+  int64_t l2_bytes() const { return l2_bytes_; }
 
   // the calling thread's lane (created or taken from the pool on first use)
   Lane& lane();
@@ -205,6 +206,7 @@ class Runtime {
   unsigned generation_ = 1;
   int device_ = 0;
   int num_sms_ = 148;
+  int64_t l2_bytes_ = 126ll << 20;
   std::mutex mu_;
   std::vector<Lane*> lanes_;
   std::map<void*, size_t> live_blocks_;
@@ -298,6 +300,11 @@ struct SparseMat {
   std::vector<int32_t> h_col;
   std::vector<T> h_val;
   std::vector<int32_t> h_perm;
+  // SpMMV kernel variant per block-width class 1, 2, 4, 8, 16, 32, set by
+  // the autotuner (pb_tune.cu); -1: the runtime default
+  int tune_tpr[6] = {-1, -1, -1, -1, -1, -1};
+  int tune_unroll[6] = {-1, -1, -1, -1, -1, -1};
+  int tune_staged[6] = {-1, -1, -1, -1, -1, -1};
 };
 
 // ----------------------------------------------------------------- helpers

@@ -1,9 +1,10 @@
 // pb_runtime.cu -- runtime (device, stream, memory cache) and the
 // type-independent part of the phist_kernels C API
 // (src/kernels/phist_kernels.h:79-185 in the PHIST sources).
-#include "pb_core.hpp"
-
 #include <chrono>
+#include <string>
+
+#include "pb_core.hpp"
 
 
 namespace pb {
@@ -36,6 +37,7 @@ void Runtime::init()
   cudaDeviceProp prop;
   PB_CUDA(cudaGetDeviceProperties(&prop, device_));
   num_sms_ = prop.multiProcessorCount;
+  if (prop.l2CacheSize > 0) l2_bytes_ = prop.l2CacheSize;
   if (const char* v = getenv("PHIST_B200_VERBOSE")) verbose = atoi(v);
   if (const char* v = getenv("PHIST_B200_TMA")) use_tma = atoi(v) != 0;
   if (const char* v = getenv("PHIST_B200_DMMA")) use_dmma = atoi(v) != 0;
@@ -529,6 +531,18 @@ void phist_b200_set_graphs(int on, int* iflag)
 {
   PB_API_BEGIN(iflag);
   rt().use_graphs = on != 0;
+  PB_API_END(iflag);
+}
+
+void phist_b200_set_option(const char* name, int value, int* iflag)
+{
+  PB_API_BEGIN(iflag);
+  PB_REQUIRE(name, PB_INVALID_INPUT, "option name is NULL");
+  const std::string o(name);
+  if (o == "tma") rt().use_tma = value != 0;
+  else if (o == "dmma") rt().use_dmma = value != 0;
+  else if (o == "graphs") rt().use_graphs = value != 0;
+  else PB_REQUIRE(false, PB_INVALID_INPUT, "unknown option '%s'", name);
   PB_API_END(iflag);
 }
 

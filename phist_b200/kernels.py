@@ -120,6 +120,7 @@ _d("phist_b200_device_memory", [_ct.POINTER(u64), _ct.POINTER(u64), c_int_p])
 _d("phist_b200_set_spmv_config", [c_int, c_int, c_int, c_int_p])
 _d("phist_b200_set_spmv_staged", [c_int, c_int_p])
 _d("phist_b200_set_graphs", [c_int, c_int_p])
+_d("phist_b200_set_option", [_ct.c_char_p, c_int, c_int_p])
 _d("phist_b200_launch_count", [_ct.POINTER(u64), c_int_p])
 _d("phist_b200_get_stream", [vpp, c_int_p])
 _d("phist_b200_problem_create", [c_char_p, c_int, gidx_p, lidx_p], vp)
@@ -160,6 +161,8 @@ for _P, _ST in (("D", _ct.c_double), ("S", _ct.c_float)):
     _d(x + "sparseMat_create_fromCRS", [vpp, vp, gidx, gidx, vp, vp, vp, c_int_p])
     _d(x + "sparseMat_sell_info", [vp, c_int_p, _ct.POINTER(_ct.c_int64), _ct.POINTER(_ct.c_int64),
                                    _ct.POINTER(_ct.c_int64), vp, c_int_p])
+    _d(x + "sparseMat_autotune", [vp, c_int, vp, c_int, vp, c_int_p])
+    _d(x + "sparseMat_get_tuning", [vp, c_int_p, _ct.POINTER(_ct.c_int64), vp, vp, vp, c_int_p])
     _d(p + "mvec_create", [vpp, vp, c_int, c_int_p])
     _d(p + "mvec_clone_shape", [vpp, vp, c_int_p])
     _d(p + "mvec_delete", [vp, c_int_p])

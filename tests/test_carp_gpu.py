@@ -146,3 +146,8 @@ def test_carp_rc_reduces_to_real(session, oracle, testmats):
     K.chk(K.phist_Dcarp_destroy, A.h, work)
     for o in (Xr, Xi, B, A):
         o.delete()
+
+
+def test_set_option_rejects_unknown_names(session):
+    from phist_b200 import kernels as K
+    assert K.iflag_of(K.phist_b200_set_option, b"no_such_option", 1) < 0
