@@ -368,7 +368,8 @@ void phist_b200_DmvecT_times_mvec_noalloc(int64_t n, int m, int k, double alpha,
  * carp_cg driver, drivers/carp_cg.c:286-320, with the CGMN recurrence of
  * src/krylov/phist_carp_cg_def.hpp:440-690 run on the GPU).  Solves
  * (A - sigma_j I) x_j = b_j for the nsys columns of B (n x nsys) into X
- * (n x nsys) through `block` (1..32) slots: each slot iterates one system;
+ * (n x nsys) through `block` (1..32) slots, or, for block <= 0, the slot
+ * count phist_b200_DcarpCG_tune_block picks: each slot iterates one system;
  * every checkEvery iterations the explicit FP64 residuals are measured, and
  * a system that reached ||b_j - (A - sigma_j I) x_j|| <= tol ||b_j|| (or
  * maxIter iterations) leaves its slot to the next queued system.  All CG
@@ -382,6 +383,13 @@ void phist_b200_DcarpCG_batch(phist_Dconst_sparseMat_ptr A, int nsys, const doub
                               phist_Dconst_mvec_ptr B, phist_Dmvec_ptr X, int block, double tol,
                               int maxIter, int checkEvery, int mixed, double innerTol, int iters[],
                               double relres[], int* iflag);
+/* slot count for phist_b200_DcarpCG_batch: the w in {1, 2, 4, 8, 16, 32},
+ * w <= max(nsys, 1), with the most system-iterations per second w / t(w),
+ * t(w) the device time of one iteration (colour sweep and fused CG updates,
+ * median of reps after a warm-up; FP32 when mixed).  iter_us[6] (may be
+ * NULL) receives t(1), t(2), ... t(32) in microseconds, 0 where not tried. */
+void phist_b200_DcarpCG_tune_block(phist_Dconst_sparseMat_ptr A, int nsys, int mixed, int reps, int* block,
+                                   double iter_us[], int* iflag);
 
 /* runtime controls and statistics (library extensions) */
 /* SELL chunk height C (1..32, power of two) and the sigma window used when a

@@ -295,9 +295,9 @@ void upload(T* d, const T* h, int w)
 // float: FP32 inner solves inside FP64 refinement).  Returns the number of
 // systems that did not converge within maxIter iterations of their slot.
 template <class TI>
-int carpcg_batch(const SparseMat<double>* A64, const SparseMat<TI>* Ain, int nsys, const double* sigma,
-                 const Mvec<double>* B, Mvec<double>* X, int w, double tol, int maxIter, int K, double innerTol,
-                 int* iters, double* relres)
+int carpcg_batch(const SparseMat<double>* A64, const SparseMat<TI>* Ain, CarpWork<TI>* work, int nsys,
+                 const double* sigma, const Mvec<double>* B, Mvec<double>* X, int w, double tol, int maxIter, int K,
+                 double innerTol, int* iters, double* relres)
 {
   constexpr bool MIXED = std::is_same<TI, float>::value;
   const int64_t n = A64->nrows;
@@ -332,11 +332,6 @@ int carpcg_batch(const SparseMat<double>* A64, const SparseMat<TI>* Ain, int nsy
   const bool flat = (256 % w) == 0;
   const int gridf = (int)std::max<int64_t>(1, std::min<int64_t>(ceil_div((int64_t)nw, 256 * 8), rt().num_sms() * 8));
 
-  CarpWork<TI>* work = carp_build<TI>(Ain, w, sigI.data(), nullptr);
-  struct WorkGuard {
-    CarpWork<TI>* w;
-    ~WorkGuard() { carp_free<TI>(w); }
-  } guard{work};
   // partial sums and arrival counter of the iteration's dots: buffers of
   // their own, so that the pointers recorded in the CUDA graph stay valid
   // whatever the lane's scratch does in between
@@ -587,17 +582,151 @@ int carpcg_batch(const SparseMat<double>* A64, const SparseMat<TI>* Ain, int nsy
   return unconverged;
 }
 
-template int carpcg_batch<double>(const SparseMat<double>*, const SparseMat<double>*, int, const double*,
-                                  const Mvec<double>*, Mvec<double>*, int, double, int, int, double, int*,
-                                  double*);
-template int carpcg_batch<float>(const SparseMat<double>*, const SparseMat<float>*, int, const double*,
-                                 const Mvec<double>*, Mvec<double>*, int, double, int, int, double, int*, double*);
+// Device time of one CGMN iteration of the batched solver for w slots (the
+// colour sweep q = dkswp(p, 0) and the fused CG updates with their column
+// dots, as in carpcg_batch) on scratch blocks: median of reps replays after
+// a warm-up, in microseconds.  The values in the blocks do not matter for
+// the time; they are set to a fixed pattern.
+template <class TI>
+double carpcg_iteration_us(const SparseMat<TI>* Ain, CarpWork<TI>* work, int w, int reps)
+{
+  const int64_t n = Ain->nrows;
+  const size_t nw = (size_t)n * w;
+  DevBuf<TI> d(nw), r(nw), p(nw), q(nw);
+  DevBuf<TI> rr(w), pq(w), alpha(w), beta(w), rrn(w);
+  DevBuf<int> active(w);
+  DevBuf<unsigned int> icnt(1);
+  const int gridf = (int)std::max<int64_t>(1, std::min<int64_t>(ceil_div((int64_t)nw, 256 * 8), rt().num_sms() * 8));
+  DevBuf<TI> ipart((size_t)gridf * w);
+  PB_CUDA(cudaMemsetAsync(icnt.p, 0, sizeof(unsigned int), stream()));
+  TI* const fill[3] = {d.p, r.p, p.p};
+  for (int k = 0; k < 3; k++)
+    k_random<TI><<<grid_for((int64_t)nw), 256, 0, stream()>>>(fill[k], w, n, w, w, 0, 77 + k);
+  PB_LAUNCH_CHECK();
+  k_put_value<TI><<<1, 32, 0, stream()>>>(rr.p, w, 1, w, TI(1));
+  k_put_value<int><<<1, 32, 0, stream()>>>(active.p, w, 1, w, 1);
+  PB_LAUNCH_CHECK();
+  std::vector<TI> sig(w, TI(0.5)), om(w, TI(1));
+  Mvec<TI> mq;
+  as_mvec(mq, q.p, n, w);
+  auto iteration = [&]() {
+    PB_CUDA(cudaMemcpyAsync(q.p, p.p, sizeof(TI) * nw, cudaMemcpyDeviceToDevice, stream()));
+    carp_run<TI, false>(work, w, sig.data(), nullptr, nullptr, &mq, nullptr, om.data());
+    k_cg_pmq_dot<TI><<<gridf, 256, 0, stream()>>>(q.p, p.p, (int64_t)nw, w, ipart.p, icnt.p, pq.p);
+    k_cg_alpha<TI><<<1, 32, 0, stream()>>>(rr.p, pq.p, active.p, alpha.p, w);
+    k_cg_xr_dot<TI><<<gridf, 256, 0, stream()>>>(d.p, r.p, p.p, q.p, alpha.p, (int64_t)nw, w, ipart.p, icnt.p,
+                                                 rrn.p);
+    k_cg_beta<TI><<<1, 32, 0, stream()>>>(rrn.p, rr.p, active.p, beta.p, w);
+    k_cg_p_flat<TI><<<gridf, 256, 0, stream()>>>(p.p, r.p, beta.p, (int64_t)nw, w);
+    PB_LAUNCH_CHECK();
+  };
+  cudaEvent_t e0, e1;
+  PB_CUDA(cudaEventCreate(&e0));
+  PB_CUDA(cudaEventCreate(&e1));
+  std::vector<float> ts;
+  try {
+    iteration();  // warm-up
+    for (int k = 0; k < std::max(1, reps); k++) {
+      PB_CUDA(cudaEventRecord(e0, stream()));
+      iteration();
+      PB_CUDA(cudaEventRecord(e1, stream()));
+      PB_CUDA(cudaEventSynchronize(e1));
+      float ms = 0.0f;
+      PB_CUDA(cudaEventElapsedTime(&ms, e0, e1));
+      ts.push_back(ms);
+    }
+  } catch (...) {
+    cudaEventDestroy(e0);
+    cudaEventDestroy(e1);
+    throw;
+  }
+  cudaEventDestroy(e0);
+  cudaEventDestroy(e1);
+  std::sort(ts.begin(), ts.end());
+  return 1e3 * (double)ts[ts.size() / 2];
+}
+
+// Slot count of the batched solver with the most system-iterations per
+// second, w / t_iteration(w), over w in {1, 2, 4, 8, 16, 32} up to nsys.
+// us[6] (may be NULL) receives each candidate's iteration time (0: not
+// tried).
+template <class TI>
+int carpcg_tune_block(const SparseMat<TI>* Ain, CarpWork<TI>* work, int nsys, int reps, double* us)
+{
+  int best = 1;
+  double best_rate = -1.0;
+  for (int k = 0; k < 6; k++) {
+    const int w = 1 << k;
+    if (us) us[k] = 0.0;
+    if (w > std::max(1, nsys)) continue;
+    const double t = carpcg_iteration_us<TI>(Ain, work, w, reps);
+    if (us) us[k] = t;
+    const double rate = w / t;
+    if (rate > best_rate) {
+      best_rate = rate;
+      best = w;
+    }
+  }
+  return best;
+}
+
+template int carpcg_batch<double>(const SparseMat<double>*, const SparseMat<double>*, CarpWork<double>*, int,
+                                  const double*, const Mvec<double>*, Mvec<double>*, int, double, int, int, double,
+                                  int*, double*);
+template int carpcg_batch<float>(const SparseMat<double>*, const SparseMat<float>*, CarpWork<float>*, int,
+                                 const double*, const Mvec<double>*, Mvec<double>*, int, double, int, int, double,
+                                 int*, double*);
 
 }  // namespace pb
 
 extern "C" {
 void phist_b200_sparseMat_DtoS(const void* vA, void** vAs, int* iflag);
 void phist_SsparseMat_delete(void* A, int* iflag);
+}
+
+namespace {
+// the FP32 copy of A for the mixed solver, deleted with the guard
+struct SCopy {
+  void* a = nullptr;
+  ~SCopy()
+  {
+    int e = 0;
+    if (a) phist_SsparseMat_delete(a, &e);
+  }
+};
+
+template <class TI>
+struct WorkGuard {
+  pb::CarpWork<TI>* w = nullptr;
+  ~WorkGuard() { pb::carp_free<TI>(w); }
+};
+}  // namespace
+
+extern "C" {
+
+void phist_b200_DcarpCG_tune_block(const void* vA, int nsys, int mixed, int reps, int* block, double* iter_us,
+                                   int* iflag)
+{
+  PB_API_BEGIN(iflag);
+  using namespace pb;
+  const SparseMat<double>* A = SP<double>(vA);
+  PB_REQUIRE(block, PB_INVALID_INPUT, "block is NULL");
+  PB_REQUIRE(A->nrows == A->ncols, PB_INVALID_INPUT, "CARP-CG needs a square matrix");
+  const float zs = 0.0f;
+  const double zd = 0.0;
+  if (mixed) {
+    SCopy s;
+    int e = 0;
+    phist_b200_sparseMat_DtoS(vA, &s.a, &e);
+    PB_REQUIRE(e == 0 && s.a, e ? e : PB_FUNCTIONAL_ERROR, "FP32 copy of the matrix failed");
+    WorkGuard<float> g{carp_build<float>(SP<float>(s.a), 1, &zs, nullptr)};
+    *block = carpcg_tune_block<float>(SP<float>(s.a), g.w, nsys, reps, iter_us);
+  } else {
+    WorkGuard<double> g{carp_build<double>(A, 1, &zd, nullptr)};
+    *block = carpcg_tune_block<double>(A, g.w, nsys, reps, iter_us);
+  }
+  PB_API_END(iflag);
+}
 
 void phist_b200_DcarpCG_batch(const void* vA, int nsys, const double* sigma, const void* vB, void* vX, int block,
                               double tol, int maxIter, int checkEvery, int mixed, double innerTol, int* iters,
@@ -608,8 +737,8 @@ void phist_b200_DcarpCG_batch(const void* vA, int nsys, const double* sigma, con
   const SparseMat<double>* A = SP<double>(vA);
   const Mvec<double>* B = MV<double>(vB);
   Mvec<double>* X = MV<double>(vX);
-  PB_REQUIRE(nsys >= 0 && block >= 1 && block <= 32, PB_INVALID_INPUT,
-             "need nsys >= 0 and 1 <= block <= 32 (got %d, %d)", nsys, block);
+  PB_REQUIRE(nsys >= 0 && block <= 32, PB_INVALID_INPUT,
+             "need nsys >= 0 and block <= 32 (got %d, %d; block <= 0: tuned)", nsys, block);
   if (nsys == 0) {
     *iflag = 0;
     return;
@@ -621,24 +750,25 @@ void phist_b200_DcarpCG_batch(const void* vA, int nsys, const double* sigma, con
   PB_REQUIRE(tol > 0.0 && maxIter > 0 && checkEvery > 0, PB_INVALID_INPUT, "tol, maxIter, checkEvery must be > 0");
   int unconverged = 0;
   if (nsys > 0) {
-    const int w = std::min(block, nsys);
+    // the colouring does not depend on the slot count or the shifts: built
+    // once, used by the block tuner (block <= 0) and the solver
+    const float zs = 0.0f;
+    const double zd = 0.0;
     if (mixed) {
-      void* As = nullptr;
+      SCopy s;
       int e = 0;
-      phist_b200_sparseMat_DtoS(vA, &As, &e);
-      PB_REQUIRE(e == 0 && As, e ? e : PB_FUNCTIONAL_ERROR, "FP32 copy of the matrix failed");
-      struct Del {
-        void* a;
-        ~Del()
-        {
-          int e2 = 0;
-          phist_SsparseMat_delete(a, &e2);
-        }
-      } del{As};
-      unconverged = carpcg_batch<float>(A, SP<float>(As), nsys, sigma, B, X, w, tol, maxIter, checkEvery,
+      phist_b200_sparseMat_DtoS(vA, &s.a, &e);
+      PB_REQUIRE(e == 0 && s.a, e ? e : PB_FUNCTIONAL_ERROR, "FP32 copy of the matrix failed");
+      const SparseMat<float>* As = SP<float>(s.a);
+      WorkGuard<float> g{carp_build<float>(As, 1, &zs, nullptr)};
+      const int w = block >= 1 ? std::min(block, nsys) : carpcg_tune_block<float>(As, g.w, nsys, 3, nullptr);
+      unconverged = carpcg_batch<float>(A, As, g.w, nsys, sigma, B, X, w, tol, maxIter, checkEvery,
                                         innerTol > 0.0 ? innerTol : 1e-5, iters, relres);
     } else {
-      unconverged = carpcg_batch<double>(A, A, nsys, sigma, B, X, w, tol, maxIter, checkEvery, tol, iters, relres);
+      WorkGuard<double> g{carp_build<double>(A, 1, &zd, nullptr)};
+      const int w = block >= 1 ? std::min(block, nsys) : carpcg_tune_block<double>(A, g.w, nsys, 3, nullptr);
+      unconverged = carpcg_batch<double>(A, A, g.w, nsys, sigma, B, X, w, tol, maxIter, checkEvery, tol, iters,
+                                         relres);
     }
   }
   *iflag = unconverged;

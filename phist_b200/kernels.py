@@ -132,6 +132,7 @@ _d("phist_b200_mvec_StoD", [vp, vp, c_int_p])
 _d("phist_b200_sparseMat_DtoS", [vp, vpp, c_int_p])
 _d("phist_b200_DcarpCG_batch",
    [vp, c_int, vp, vp, vp, c_int, _ct.c_double, c_int, c_int, c_int, _ct.c_double, vp, vp, c_int_p])
+_d("phist_b200_DcarpCG_tune_block", [vp, c_int, c_int, c_int, c_int_p, vp, c_int_p])
 _d("phist_b200_DmvecT_times_mvec_noalloc",
    [gidx, c_int, c_int, _ct.c_double, vp, gidx, vp, gidx, _ct.c_double, vp, gidx, vp, c_int_p])
 

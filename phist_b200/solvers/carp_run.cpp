@@ -22,7 +22,8 @@
 //         batch=1: the library's batched solver phist_b200_DcarpCG_batch
 //         instead of PHIST's carp_cgState (block = slots, converged systems
 //         refilled from the queue, checks every checkEvery (10) iterations;
-//         mixed=1 there means FP32 inner solves with FP64 refinement)
+//         mixed=1 there means FP32 inner solves with FP64 refinement;
+//         block=0 there: slot count from phist_b200_DcarpCG_tune_block)
 //   shifts sigma_j = 2.5 * u(seed, j), right-hand sides b_ij = u(seed + 1 + j, i)
 //   with u uniform [-1,1) from a splitmix64 hash (the library's pb_unif).
 #include <algorithm>
@@ -51,6 +52,8 @@ void phist_b200_DcarpCG_batch(phist_Dconst_sparseMat_ptr A, int nsys, const doub
                               phist_Dconst_mvec_ptr B, phist_Dmvec_ptr X, int block, double tol,
                               int maxIter, int checkEvery, int mixed, double innerTol, int iters[],
                               double relres[], int* iflag);
+void phist_b200_DcarpCG_tune_block(phist_Dconst_sparseMat_ptr A, int nsys, int mixed, int reps, int* block,
+                                   double iter_us[], int* iflag);
 }
 
 #define CHK(call)                                                              \
@@ -119,7 +122,7 @@ int main(int argc, char** argv)
     else if (k == "batch") batch = atoi(v);
     else if (k == "checkEvery") checkEvery = atoi(v);
   }
-  if (block < 1 || nshifts < 1) return 2;
+  if (block < (batch ? 0 : 1) || nshifts < 1) return 2;
 
   CHK(phist_kernels_init(&argc, &argv, &iflag));
   phist_comm_ptr comm = NULL;
@@ -145,6 +148,11 @@ int main(int argc, char** argv)
     for (phist_lidx i = 0; i < nloc; i++)
       for (int j = 0; j < nshifts; j++) h[(size_t)i * nshifts + j] = unif(seed + 1 + j, (uint64_t)i);
     CHK(phist_Dmvec_set_data(B, h.data(), nshifts, 1, &iflag));
+  }
+
+  std::vector<double> iter_us(6, 0.0);
+  if (block == 0) {
+    CHK(phist_b200_DcarpCG_tune_block(A, nshifts, mixed, 3, &block, iter_us.data(), &iflag));
   }
 
   std::vector<double> walls, relres(nshifts, 0.0);
@@ -236,6 +244,8 @@ int main(int argc, char** argv)
   for (size_t i = 0; i < refines.size(); i++) printf("%s%d", i ? ", " : "", refines[i]);
   printf("], \"fp64_refinements\": [");
   for (size_t i = 0; i < fp64_steps.size(); i++) printf("%s%d", i ? ", " : "", fp64_steps[i]);
+  printf("], \"tuned_iter_us\": [");
+  for (int k = 0; k < 6; k++) printf("%s%.2f", k ? ", " : "", iter_us[k]);
   printf("], \"n\": %d, \"nshifts\": %d, \"block\": %d, \"tol\": %.3e, \"maxIter\": %d, "
          "\"omega\": %g, \"nconv\": %d, \"launches\": %llu, \"max_relres\": ",
          nloc, nshifts, block, tol, maxIter, omega, nconv, (unsigned long long)launches);

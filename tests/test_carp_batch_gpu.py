@@ -96,3 +96,29 @@ def test_batch_graph_replay_is_bitwise_identical(session, mixed):
     np.testing.assert_array_equal(it0, it1)
     np.testing.assert_array_equal(x0, x1)
     np.testing.assert_array_equal(rel0, rel1)
+
+
+@pytest.mark.parametrize("mixed", [0, 1])
+def test_block_tuner_and_auto_block(session, mixed):
+    """the slot-count tuner times widths 1..min(32, nsys) and picks one of
+    them; block <= 0 solves with that count and gives the same bits as
+    passing the count explicitly"""
+    import ctypes as ct
+
+    from phist_b200 import generators as G
+    from phist_b200 import kernels as K
+    from phist_b200.objects import SparseMat
+    rp, c, v = G.problem("HONEYCOMB-16x12-S2-W1")
+    A = SparseMat.from_crs(rp, c, v)
+    nsys = 6
+    blk = ct.c_int()
+    us = np.zeros(6)
+    K.chk(K.phist_b200_DcarpCG_tune_block, A.h, nsys, mixed, 2, ct.byref(blk), K.ptr(us))
+    A.delete()
+    assert blk.value in (1, 2, 4)
+    assert (us[:3] > 0).all() and (us[3:] == 0).all()
+    *_, x0, it0, rel0, f0 = _run("HONEYCOMB-16x12-S2-W1", nsys, 0, mixed)
+    *_, x1, it1, rel1, f1 = _run("HONEYCOMB-16x12-S2-W1", nsys, blk.value, mixed)
+    assert f0 == f1 == 0
+    np.testing.assert_array_equal(it0, it1)
+    np.testing.assert_array_equal(x0, x1)
