@@ -391,6 +391,28 @@ void phist_b200_DcarpCG_batch(phist_Dconst_sparseMat_ptr A, int nsys, const doub
 void phist_b200_DcarpCG_tune_block(phist_Dconst_sparseMat_ptr A, int nsys, int mixed, int reps, int* block,
                                    double iter_us[], int* iflag);
 
+/* Device-resident GMRES for the Jacobi-Davidson correction equations
+ *   (I - Q Q')(A - sigma_j I) t_j = res(:, resIndex[j]),  j < k <= 32
+ * (the task of PHIST's jadaCorrectionSolver_run with GMRES,
+ * src/jada/phist_jadaCorrectionSolver_def.hpp:141-583).  Q (n x nq, may be
+ * NULL) has orthonormal columns; resIndex may be NULL (identity).  x_0 = 0;
+ * restarted after maxBas steps (<= 63), at most maxIter steps; system j is
+ * converged when its GMRES residual is below 1000 eps absolute or tol[j]
+ * relative to ||res_j|| (phist_blockedgmres_def.hpp:604-606).  The
+ * Hessenberg matrices, rotations and all dot products stay on the device;
+ * Gram-Schmidt is classical, done twice, as block products.  t (n x k)
+ * receives the solutions scaled to unit norm (as PHIST returns them);
+ * *iflag >= 0 is the number of systems that did not converge.  The S form
+ * runs in FP32 (the small dense part in FP64). */
+void phist_b200_DjadaCorrection_gmres(phist_Dconst_sparseMat_ptr A, phist_Dconst_mvec_ptr Q,
+                                      phist_Dconst_mvec_ptr res, const int resIndex[], int k,
+                                      const double sigma[], const double tol[], int maxIter, int maxBas,
+                                      phist_Dmvec_ptr t, int* iflag);
+void phist_b200_SjadaCorrection_gmres(phist_Sconst_sparseMat_ptr A, phist_Sconst_mvec_ptr Q,
+                                      phist_Sconst_mvec_ptr res, const int resIndex[], int k,
+                                      const double sigma[], const double tol[], int maxIter, int maxBas,
+                                      phist_Smvec_ptr t, int* iflag);
+
 /* runtime controls and statistics (library extensions) */
 /* SELL chunk height C (1..32, power of two) and the sigma window used when a
  * matrix is built with PHIST_SPARSEMAT_PERM_LOCAL (<=1: no sorting) */

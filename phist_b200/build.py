@@ -25,7 +25,8 @@ LIBNAME = "libphist_kernels_b200.so"
 LIBPATH = os.path.join(LIBDIR, LIBNAME)
 
 SOURCES = ["pb_runtime.cu", "pb_api_D.cu", "pb_api_S.cu", "pb_api_mixed.cu", "pb_matfuncs.cu",
-           "pb_noalloc.cu", "pb_carpcg.cu", "pb_tune.cu"]
+           "pb_noalloc.cu", "pb_carpcg.cu", "pb_tune.cu",
+           "pb_gmres.cu"]
 ARCH = ["-gencode", "arch=compute_100a,code=sm_100a"]
 NVCC_FLAGS = ["-O3", "-lineinfo", "-std=c++17", "-Xcompiler", "-fPIC,-O3",
               "--expt-relaxed-constexpr", "-diag-suppress", "550,177"]

@@ -18,6 +18,8 @@
 //         mixed=1 (FP32 correction equations through pb_mixed_jada.h; the
 //         outer iteration, Rayleigh-Ritz, orthogonalisation and residuals
 //         stay FP64)
+//         devgmres=1 (correction equations on the library's device-resident
+//         GMRES, FP64, or FP32 with mixed=1)
 #include <chrono>
 #include <cmath>
 #include <cstdio>
@@ -89,7 +91,7 @@ int main(int argc, char** argv)
   uint64_t seed = 0;
   int64_t sigma = 1;
   int reps = 1;
-  int mixed = 0;
+  int mixed = 0, devgmres = 0;
   for (int a = 2; a < argc; a++) {
     const char* kv = argv[a];
     const char* eq = strchr(kv, '=');
@@ -113,6 +115,7 @@ int main(int argc, char** argv)
     else if (k == "sigma") sigma = atoll(v);
     else if (k == "reps") reps = atoi(v);
     else if (k == "mixed") mixed = atoi(v);
+    else if (k == "devgmres") devgmres = atoi(v);
   }
 
   CHK(phist_kernels_init(&argc, &argv, &iflag));
@@ -134,8 +137,8 @@ int main(int argc, char** argv)
   CHK(phist_map_get_local_length(map, &nloc, &iflag));
 
   pb_mixed_jada* mixedSolver = NULL;
-  if (mixed) {
-    CHK(phist_b200_mixed_jada_create(&mixedSolver, A, &opts, &iflag));
+  if (mixed || devgmres) {
+    CHK(phist_b200_jada_inner_create(&mixedSolver, A, &opts, mixed ? 1 : 0, devgmres, &iflag));
     CHK(phist_b200_mixed_jada_install(mixedSolver, &opts, &iflag));
   }
 
@@ -196,11 +199,11 @@ int main(int argc, char** argv)
   }
   long mcalls = 0, msys = 0, munconv = 0;
   if (mixedSolver) CHK(phist_b200_mixed_jada_stats(mixedSolver, &mcalls, &msys, &munconv, &iflag));
-  printf("{\"problem\": \"%s\", \"mixed\": %d, \"inner_calls\": %ld, \"inner_systems\": %ld, "
+  printf("{\"problem\": \"%s\", \"mixed\": %d, \"devgmres\": %d, \"inner_calls\": %ld, \"inner_systems\": %ld, "
          "\"inner_unconverged\": %ld, \"n\": %d, \"numEigs\": %d, \"blockSize\": %d, \"minBas\": %d, "
          "\"maxBas\": %d, \"convTol\": %.3e, \"nConv\": %d, \"nIter\": %d, \"t_create\": %.4f, "
          "\"launches\": %llu, \"wall\": [",
-         problem, mixed, mcalls, msys, munconv, nloc, nEig, bs, opts.minBas, opts.maxBas, opts.convTol, nConv, nIter, t_create,
+         problem, mixed, devgmres, mcalls, msys, munconv, nloc, nEig, bs, opts.minBas, opts.maxBas, opts.convTol, nConv, nIter, t_create,
          (unsigned long long)launches);
   for (size_t i = 0; i < walls.size(); i++) printf("%s%.6f", i ? ", " : "", walls[i]);
   printf("], \"ev\": [");

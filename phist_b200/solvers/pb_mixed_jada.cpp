@@ -22,6 +22,12 @@
 #include "pb_mixed_jada.h"
 
 extern "C" {
+void phist_b200_DjadaCorrection_gmres(phist_Dconst_sparseMat_ptr A, phist_Dconst_mvec_ptr Q,
+                                      phist_Dconst_mvec_ptr res, const int resIndex[], int k, const double sigma[],
+                                      const double tol[], int maxIter, int maxBas, phist_Dmvec_ptr t, int* iflag);
+void phist_b200_SjadaCorrection_gmres(phist_Sconst_sparseMat_ptr A, phist_Sconst_mvec_ptr Q,
+                                      phist_Sconst_mvec_ptr res, const int resIndex[], int k, const double sigma[],
+                                      const double tol[], int maxIter, int maxBas, phist_Smvec_ptr t, int* iflag);
 void phist_b200_mvec_DtoS(phist_Dconst_mvec_ptr X, phist_Smvec_ptr Y, int* iflag);
 void phist_b200_mvec_StoD(phist_Sconst_mvec_ptr X, phist_Dmvec_ptr Y, int* iflag);
 void phist_b200_sparseMat_DtoS(phist_Dconst_sparseMat_ptr A, phist_SsparseMat_ptr* As, int* iflag);
@@ -60,6 +66,10 @@ struct WorkBlock {
 }  // namespace
 
 struct pb_mixed_jada {
+  int fp32 = 1;         // correction equations in FP32 (else FP64)
+  int devgmres = 0;     // the library's device-resident GMRES (else PHIST's blocked GMRES)
+  int maxBas = 20;      // GMRES basis size of the device solver
+  phist_Dconst_sparseMat_ptr A = nullptr;
   phist_SsparseMat_ptr As = nullptr;
   phist_SlinearOp opAs;
   phist_SjadaCorrectionSolver_ptr inner = nullptr;
@@ -97,6 +107,21 @@ static void pb_mixed_jada_run(void* data, void const* A_op, void const* B_op, vo
       *iflag = PHIST_NOT_IMPLEMENTED;  // complex shifts need the complex FP32 path
       return;
     }
+  if (k > 64) {
+    *iflag = PHIST_INVALID_INPUT;
+    return;
+  }
+  if (!me->fp32) {
+    // FP64 on the device-resident GMRES: no conversions
+    *iflag = 0;
+    phist_b200_DjadaCorrection_gmres(me->A, (phist_Dconst_mvec_ptr)Qtil, (phist_Dconst_mvec_ptr)res, resIndex, k,
+                                     sigma_r, tol, maxIter, me->maxBas, (phist_Dmvec_ptr)t, iflag);
+    if (*iflag < 0) return;
+    me->calls++;
+    me->systems += k;
+    me->unconverged += *iflag;
+    return;
+  }
 
   PB_CHK(me->Q.view(me->map, nq, iflag));
   PB_CHK(me->R.view(me->map, nres, iflag));
@@ -118,18 +143,19 @@ static void pb_mixed_jada_run(void* data, void const* A_op, void const* B_op, vo
     PB_CHK(phist_Smvec_vscale(me->R.v, sc.data(), iflag));
   }
 
-  float s[64], tl[64];
-  if (k > 64) {
-    *iflag = PHIST_INVALID_INPUT;
-    return;
-  }
-  for (int j = 0; j < k; j++) {
-    s[j] = (float)sigma_r[j];
-    tl[j] = (float)tol[j];
-  }
   *iflag = 0;
-  phist_SjadaCorrectionSolver_run(me->inner, &me->opAs, nullptr, me->Q.v, nullptr, s, me->R.v, resIndex, tl,
-                                  maxIter, me->T.v, robust, abortAfterFirstConvergedInBlock, 0, iflag);
+  if (me->devgmres) {
+    phist_b200_SjadaCorrection_gmres(me->As, me->Q.v, me->R.v, resIndex, k, sigma_r, tol, maxIter, me->maxBas,
+                                      me->T.v, iflag);
+  } else {
+    float s[64], tl[64];
+    for (int j = 0; j < k; j++) {
+      s[j] = (float)sigma_r[j];
+      tl[j] = (float)tol[j];
+    }
+    phist_SjadaCorrectionSolver_run(me->inner, &me->opAs, nullptr, me->Q.v, nullptr, s, me->R.v, resIndex, tl,
+                                    maxIter, me->T.v, robust, abortAfterFirstConvergedInBlock, 0, iflag);
+  }
   if (*iflag < 0) return;
   const int notConverged = *iflag;
   PB_CHK(phist_b200_mvec_StoD(me->T.v, (phist_Dmvec_ptr)t, iflag));
@@ -141,6 +167,12 @@ static void pb_mixed_jada_run(void* data, void const* A_op, void const* B_op, vo
 
 extern "C" void phist_b200_mixed_jada_create(pb_mixed_jada** out, void const* A, const phist_jadaOpts* opts,
                                              int* iflag)
+{
+  phist_b200_jada_inner_create(out, A, opts, 1, 0, iflag);
+}
+
+extern "C" void phist_b200_jada_inner_create(pb_mixed_jada** out, void const* A, const phist_jadaOpts* opts,
+                                             int fp32, int devgmres, int* iflag)
 {
   *iflag = 0;
   if (!out || !A || !opts) {
@@ -156,10 +188,18 @@ extern "C" void phist_b200_mixed_jada_create(pb_mixed_jada** out, void const* A,
     *iflag = PHIST_MEM_ALLOC_FAILED;
     return;
   }
+  me->fp32 = fp32 ? 1 : 0;
+  me->devgmres = (devgmres || !fp32) ? 1 : 0;  // FP64 here means the device GMRES
+  me->maxBas = opts->innerSolvMaxBas > 0 ? opts->innerSolvMaxBas : opts->innerSolvMaxIters;
+  me->A = (phist_Dconst_sparseMat_ptr)A;
+  if (!me->fp32) {
+    *out = me;
+    return;
+  }
   phist_b200_sparseMat_DtoS((phist_Dconst_sparseMat_ptr)A, &me->As, iflag);
   if (*iflag == 0) phist_SlinearOp_wrap_sparseMat(&me->opAs, me->As, iflag);
   if (*iflag == 0) phist_SsparseMat_get_domain_map(me->As, &me->map, iflag);
-  if (*iflag == 0) {
+  if (*iflag == 0 && !me->devgmres) {
     phist_jadaOpts o = *opts;
     o.customSolver = nullptr;
     o.customSolver_run = nullptr;

@@ -41,6 +41,18 @@ typedef struct pb_mixed_jada pb_mixed_jada;
  * are handled; run() answers anything else with -99 (PHIST_NOT_IMPLEMENTED). */
 void phist_b200_mixed_jada_create(pb_mixed_jada** me, void const* A, const phist_jadaOpts* opts, int* iflag);
 
+/* The general form: fp32 = 1 solves the correction equations in FP32 (on
+ * the FP32 copy of A), fp32 = 0 in FP64 (on A itself); devgmres = 1 uses the
+ * library's device-resident GMRES (phist_b200_{D,S}jadaCorrection_gmres:
+ * Hessenberg matrix, rotations and every dot product on the GPU, CGS2 as
+ * block products, no host synchronisation per step) instead of PHIST's
+ * blocked GMRES.  fp32 = 0 always means the device GMRES (PHIST's own FP64
+ * GMRES is what subspacejada runs without this hook).  GMRES basis size:
+ * innerSolvMaxBas, or innerSolvMaxIters when that is < 0 (PHIST's rule,
+ * src/jada/phist_jadaCorrectionSolver_def.hpp:37-38). */
+void phist_b200_jada_inner_create(pb_mixed_jada** me, void const* A, const phist_jadaOpts* opts, int fp32,
+                                  int devgmres, int* iflag);
+
 /* Points opts at this solver: innerSolvType = phist_USER_LINSOLV,
  * customSolver = me, customSolver_run = the FP32 solve. */
 void phist_b200_mixed_jada_install(pb_mixed_jada* me, phist_jadaOpts* opts, int* iflag);

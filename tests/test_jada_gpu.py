@@ -149,3 +149,25 @@ def test_subspacejada_anderson(session, mixed):
     ev = np.sort(np.asarray(r["ev"][:nev]))
     assert np.abs(ev - lam[:nev]).max() <= tol * rho, (ev, lam[:nev])
     assert max(r["resExplicit"][:nev]) < 20 * tol
+
+
+@pytest.mark.parametrize("L", [12, 16])
+def test_subspacejada_device_gmres(session, L):
+    """correction equations on the library's device-resident GMRES (FP64, and
+    FP32 with mixed=1): the same 10 smallest eigenpairs to the same
+    tolerance; FP64 within 10 % (+2) of the outer iterations of PHIST's own
+    GMRES, FP32 within the mixed form's bound"""
+    tol, seed = 1e-10, 3
+    args = ["LAPDIAG3D-%d-S%d" % (L, seed), "numEigs=10", "blockSize=4", "minBas=20", "maxBas=40",
+            "convTol=%g" % tol, "which=SR"]
+    r64 = run(*args)
+    rd = run(*(args + ["devgmres=1"]))
+    rm = run(*(args + ["devgmres=1", "mixed=1"]))
+    exact, rho = lapdiag_eigs(L, seed, 10)
+    for r in (rd, rm):
+        assert r["devgmres"] == 1 and r["inner_calls"] > 0
+        assert r["nConv"] >= 10
+        assert np.abs(np.sort(r["ev"][:10]) - exact).max() <= tol * rho, (r["mixed"], r["ev"][:10], exact)
+        assert max(r["resExplicit"][:10]) < 20 * tol
+    assert rd["nIter"] <= 1.1 * r64["nIter"] + 2, (rd["nIter"], r64["nIter"])
+    assert rm["nIter"] <= 1.5 * r64["nIter"] + 5, (rm["nIter"], r64["nIter"])

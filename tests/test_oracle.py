@@ -204,3 +204,43 @@ def test_dist2_checker(oracle):
     n = len(rp) - 1
     assert oracle.check_dist2(rp, c, n, np.arange(n)) == 0       # all distinct
     assert oracle.check_dist2(rp, c, n, np.zeros(n)) != 0        # all equal
+
+
+def test_oracle_jada_gmres_is_the_krylov_minimiser():
+    """the numpy restatement of PHIST's correction-equation GMRES: after j
+    steps its iterate minimises ||b - P(A - sigma I) x|| over the Krylov
+    space of b (checked by dense least squares); with a large enough basis it
+    converges; the result has unit norm"""
+    from oracle import oracle as O
+    rng = np.random.default_rng(0)
+    n = 60
+    A = rng.standard_normal((n, n))
+    A = A + A.T + 10 * np.eye(n)
+    Q = np.linalg.qr(rng.standard_normal((n, 3)))[0]
+    R = rng.standard_normal((n, 2))
+    R -= Q @ (Q.T @ R)
+    P = np.eye(n) - Q @ Q.T
+    for j in (1, 3, 7):
+        t, conv = O.jada_gmres(A, Q, R[:, :1], [0.5], [1e-30], j, 20)
+        op = P @ (A - 0.5 * np.eye(n))
+        # an orthonormal basis of the Krylov space (the power basis is too
+        # ill-conditioned for a tight comparison)
+        K = np.zeros((n, j))
+        v = R[:, 0] / np.linalg.norm(R[:, 0])
+        for i in range(j):
+            K[:, i] = v
+            v = op @ v
+            v -= K[:, :i + 1] @ (K[:, :i + 1].T @ v)
+            v -= K[:, :i + 1] @ (K[:, :i + 1].T @ v)
+            v /= np.linalg.norm(v)
+        c, *_ = np.linalg.lstsq(op @ K, R[:, 0], rcond=None)
+        x = K @ c
+        assert not conv[0]
+        assert np.linalg.norm(t[:, 0] - x / np.linalg.norm(x)) < 1e-10
+    t, conv = O.jada_gmres(A, Q, R, [0.5, 1.0], [1e-10, 1e-10], 200, 60)
+    assert conv.all()
+    assert np.allclose(np.linalg.norm(t, axis=0), 1.0)
+    for s, sg in enumerate((0.5, 1.0)):
+        y = P @ (A - sg * np.eye(n)) @ t[:, s]
+        a = (y @ R[:, s]) / (y @ y)
+        assert np.linalg.norm(a * y - R[:, s]) < 1e-9 * np.linalg.norm(R[:, s])
