@@ -14,9 +14,9 @@
 // block products per pass: C = [V_0..V_j]' W on the tensor-core mvTmv
 // kernels, then W -= [V_0..V_j] D with D the block-diagonal part of C
 // (system s only uses the coefficients of its own column).  An iteration is
-// ~15 asynchronous launches with no host synchronisation; the host stays at
-// most two iterations ahead of the device by reading an iteration counter
-// the device writes into mapped host memory, and stops early once every
+// ~15 asynchronous launches with no host synchronisation; after each step
+// the host looks (without waiting) at a step counter and converged count the
+// device writes into mapped host memory, and stops launching once every
 // system has converged.
 //
 // The arithmetic of the GMRES iterate is PHIST's: x_0 = 0, Krylov space of
@@ -27,7 +27,6 @@
 // unit norm (phist_jadaCorrectionSolver_def.hpp:576-578).  The small dense
 // part (Hessenberg, rotations, triangular solve) is FP64 in both precisions.
 #include <algorithm>
-#include <chrono>
 #include <cmath>
 #include <limits>
 #include <vector>
@@ -341,17 +340,10 @@ int jada_gmres(const SparseMat<T>* A, const Mvec<T>* Q, const Mvec<T>* R, const 
       k_gm_scale_cols<T><<<gw, 256, 0, stream()>>>(W.p, k, V.p + (int64_t)(j + 1) * k, ldV, n, k, f.p);
       PB_LAUNCH_CHECK();
       steps = j + 1;
-      // stay at most two steps ahead of the device; stop once all converged
-      if (j >= 2) {
-        const auto t0 = std::chrono::steady_clock::now();
-        while (hflags[0] < j - 2) {
-          if (std::chrono::steady_clock::now() - t0 > std::chrono::seconds(30)) {
-            rt().sync();  // reports a device error, if any
-            PB_REQUIRE(false, PB_FUNCTIONAL_ERROR, "GMRES step %d did not complete", j - 2);
-          }
-        }
-        if (hflags[1] >= k) stop = true;
-      }
+      // stop launching once the device reports every system converged (a
+      // look at the flags, no wait: the host never blocks inside a cycle,
+      // so concurrent solves on other threads keep their cores)
+      if (hflags[0] >= 0 && hflags[1] >= k) stop = true;
     }
     total += steps;
     // x += [V_0..V_{J-1}] y with J the largest step count of a system

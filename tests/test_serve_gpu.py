@@ -37,11 +37,11 @@ def lapdiag_eigs(L, seed, k):
     return np.linalg.eigvalsh(A)[:k], np.abs(np.linalg.eigvalsh(A)).max()
 
 
-@pytest.mark.parametrize("mixed", [0, 1])
-def test_served_stream_matches_alone_and_spectrum(session, mixed):
+@pytest.mark.parametrize("mixed,devgmres", [(0, 0), (1, 0), (0, 1), (1, 1)])
+def test_served_stream_matches_alone_and_spectrum(session, mixed, devgmres):
     tol = 1e-10
     common = ["nreq=6", "rate=500", "lmin=8", "lmax=12", "seed=5", "numEigs=6", "blockSize=2", "minBas=12",
-              "maxBas=24", "tol=%g" % tol, "mixed=%d" % mixed]
+              "maxBas=24", "tol=%g" % tol, "mixed=%d" % mixed, "devgmres=%d" % devgmres]
     mix = run(*(common + ["workers=3"]))
     assert mix["failed"] == 0 and mix["unconverged"] == 0
     assert mix["max_resExplicit"] < 20 * tol
