@@ -139,16 +139,16 @@ __global__ void k_gm_extract(const T* __restrict__ C, int ldc, int j, int k, int
 // 0 then publishes (number converged, j) in mapped host memory, the count
 // first.
 template <class T>
-__global__ void k_gm_step(const T* __restrict__ G, int j, int k, int m, double* H, double* cs, double* sn, double* g,
-                          const double* __restrict__ bnorm, T* f, int* conv, int* jcount, double eps_abs, GmTol tol,
-                          volatile int* flags)
+__global__ void k_gm_step(const T* __restrict__ G, int gstride, int j, int k, int m, double* H, double* cs, double* sn,
+                          double* g, const double* __restrict__ bnorm, T* f, int* conv, int* jcount, double eps_abs,
+                          GmTol tol, volatile int* flags)
 {
   const int s = threadIdx.x;
   __shared__ int nconv;
   if (s == 0) nconv = 0;
   __syncthreads();
   if (s < k) {
-    const double hn = sqrt(fmax((double)G[s + s * k], 0.0));
+    const double hn = sqrt(fmax((double)G[s * gstride], 0.0));
     auto Hat = [&](int i) -> double& { return H[((int64_t)i * m + j) * k + s]; };
     for (int i = 0; i < j; i++) {
       const double a = Hat(i), b = Hat(i + 1);
@@ -217,6 +217,126 @@ __global__ void k_gm_invnorm(const T* __restrict__ G, int k, T* f)
   f[s] = nr > 0.0 ? (T)(1.0 / nr) : T(0);
 }
 
+// Row-parallel Gram-Schmidt kernels for J = j+1 <= GM_MAXJ basis blocks
+// and (J+1)*k <= GM_MAXOUT outputs.
+// Thread (row r, system s) with s = tid % KP (KP = k rounded up to a power
+// of two) walks rows with a grid stride.
+//   UPD:  w_s <- w_s - sum_i V(r, i*k+s) h[i*k+s]   (h on the device)
+//   DOTS: out[i*k+s] = sum_r V(r, i*k+s) w_s(r) for i < J, and
+//         out[J*k+s] = sum_r w_s(r)^2 (of w after the update, if any);
+//         without DOTS only out[s] = ||w_s||^2.
+// skip (may be NULL): the kernel does nothing when *skip == 0.
+// Sums: butterfly over the lanes of one system, warps in order, then the
+// fixed-order last-block pass: bitwise reproducible.
+constexpr int GM_MAXJ = 24;
+constexpr int GM_MAXOUT = 256;  // (J+1)*k outputs at most
+
+template <class T, bool UPD, bool DOTS, int KP>
+__global__ void __launch_bounds__(256) k_gm_rows(int64_t n, int k, int J, const T* __restrict__ V, int64_t ldV, T* W,
+                                                 const T* __restrict__ h, const int* __restrict__ skip, T* part,
+                                                 unsigned int* counter, T* out)
+{
+  if (skip && *skip == 0) return;
+  constexpr int NA = DOTS ? GM_MAXJ + 1 : 1;
+  const int tid = threadIdx.x, s = tid % KP;
+  const int nout = DOTS ? (J + 1) * k : k;
+  T acc[NA];
+#pragma unroll
+  for (int i = 0; i < NA; i++) acc[i] = T(0);
+  if (s < k) {
+    const int64_t rstep = (int64_t)gridDim.x * (256 / KP);
+    for (int64_t r = blockIdx.x * (int64_t)(256 / KP) + tid / KP; r < n; r += rstep) {
+      const T* vr = V + r * ldV + s;
+      T w = W[r * k + s];
+      if (UPD) {
+#pragma unroll 4
+        for (int i = 0; i < J; i++) w -= vr[(int64_t)i * k] * __ldg(h + i * k + s);
+        W[r * k + s] = w;
+      }
+      if (DOTS) {
+#pragma unroll
+        for (int i = 0; i < GM_MAXJ; i++)
+          if (i < J) acc[i] += vr[(int64_t)i * k] * w;
+        acc[GM_MAXJ] += w * w;
+      } else {
+        acc[0] += w * w;
+      }
+    }
+  }
+  // lanes of one system: xor over the lane bits above log2(KP)
+#pragma unroll
+  for (int i = 0; i < NA; i++)
+#pragma unroll
+    for (int off = 16; off >= KP; off >>= 1) acc[i] += __shfl_xor_sync(0xffffffffu, acc[i], off);
+  __shared__ T red[8][GM_MAXOUT];
+  const int lane = tid & 31, warp = tid >> 5;
+  if (lane < KP && s < k) {
+    if (DOTS) {
+#pragma unroll
+      for (int i = 0; i < GM_MAXJ; i++)
+        if (i < J) red[warp][i * k + s] = acc[i];
+      red[warp][J * k + s] = acc[GM_MAXJ];
+    } else {
+      red[warp][s] = acc[0];
+    }
+  }
+  __syncthreads();
+  for (int o = tid; o < nout; o += 256) {
+    T v = T(0);
+    for (int w8 = 0; w8 < 8; w8++) v += red[w8][o];
+    part[(int64_t)blockIdx.x * nout + o] = v;
+  }
+  last_block_reduce<T>(part, nout, gridDim.x, counter, out, 1, nout, 0, T(1), T(0));
+}
+
+// After pass 1: O1 = (h1, ||w||^2 before), O2 = (h2, ||w||^2 after).  H(:, j)
+// = h1 (+ h2 when a second pass follows).  The second pass runs (flag 1)
+// when some system's norm fell below 1/sqrt(2) of its value before the
+// pass (the "twice is enough" test); otherwise Nf takes the norms after
+// pass 1 and the second-pass kernel is skipped.
+template <class T>
+__global__ void k_gm_decide(const T* __restrict__ O1, const T* __restrict__ O2, int J, int k, int m, int j, double* H,
+                            T* Nf, int* reorth)
+{
+  __shared__ int any;
+  const int s = threadIdx.x;
+  if (s == 0) any = 0;
+  __syncthreads();
+  if (s < k) {
+    const double before = (double)O1[J * k + s], after = (double)O2[J * k + s];
+    if (after < 0.5 * before) atomicOr(&any, 1);
+  }
+  __syncthreads();
+  if (s < k) {
+    for (int i = 0; i < J; i++)
+      H[((int64_t)i * m + j) * k + s] = (double)O1[i * k + s] + (any ? (double)O2[i * k + s] : 0.0);
+    if (!any) Nf[s] = O2[J * k + s];
+  }
+  if (s == 0) *reorth = any;
+}
+
+template <class T, bool UPD, bool DOTS>
+void gm_rows(int64_t n, int k, int J, const T* V, int64_t ldV, T* W, const T* h, const int* skip, T* out)
+{
+  const int KP = k <= 1 ? 1 : k <= 2 ? 2 : k <= 4 ? 4 : k <= 8 ? 8 : k <= 16 ? 16 : 32;
+  const int rows_per_block = 256 / KP;
+  const int grid = (int)std::max<int64_t>(1, std::min<int64_t>(ceil_div(n, rows_per_block), rt().num_sms() * 4));
+  const int nout = DOTS ? (J + 1) * k : k;
+  T* part = (T*)rt().scratch(sizeof(T) * (size_t)grid * nout);
+#define PB_GMR(KPv)                                                                                         \
+  k_gm_rows<T, UPD, DOTS, KPv><<<grid, 256, 0, stream()>>>(n, k, J, V, ldV, W, h, skip, part, rt().counters(), out)
+  switch (KP) {
+    case 1: PB_GMR(1); break;
+    case 2: PB_GMR(2); break;
+    case 4: PB_GMR(4); break;
+    case 8: PB_GMR(8); break;
+    case 16: PB_GMR(16); break;
+    default: PB_GMR(32); break;
+  }
+#undef PB_GMR
+  PB_LAUNCH_CHECK();
+}
+
 }  // namespace
 
 // W = alpha V C + beta W on device operands (C col-major m x k, ld ldc)
@@ -266,7 +386,8 @@ int jada_gmres(const SparseMat<T>* A, const Mvec<T>* Q, const Mvec<T>* R, const 
   DBuf<T> C((size_t)(m + 1) * k * k), D((size_t)(m + 1) * k * k), Cq((size_t)std::max(nq, 1) * k);
   DBuf<T> Gk((size_t)k * k), f(k);
   DBuf<double> H((size_t)(m + 1) * m * k), cs((size_t)m * k), sn((size_t)m * k), g((size_t)(m + 1) * k), bnorm(k);
-  DBuf<int> conv(k), jcount(k);
+  DBuf<int> conv(k), jcount(k), reorth(1);
+  DBuf<T> O1((size_t)(GM_MAXJ + 1) * k), O2((size_t)(GM_MAXJ + 1) * k), Nf(k);
   GmIndex gi;
   GmTol gt;
   for (int s = 0; s < k; s++) {
@@ -325,17 +446,36 @@ int jada_gmres(const SparseMat<T>* A, const Mvec<T>* Q, const Mvec<T>* R, const 
       raw_view(mVj, V.p + (int64_t)j * k, n, k, ldV);
       spmv_general<T>(T(1), A, negsig.data(), &mVj, T(0), &mW, nullptr, nullptr, T(0), T(0), nullptr);
       project();
-      // CGS2 against V_0..V_j
+      // Gram-Schmidt against V_0..V_j
       const int rows = (j + 1) * k;
-      for (int pass = 0; pass < 2; pass++) {
-        launch_mvTmv<T>(n, rows, k, T(1), V.p, ldV, W.p, k, T(0), C.p, rows);
-        k_gm_extract<T><<<std::max(1, (rows * k + 255) / 256), 256, 0, stream()>>>(C.p, rows, j, k, m, H.p, D.p, pass);
+      const T* nrm_p = Gk.p;
+      int nrm_stride = k + 1;
+      if (j + 1 <= GM_MAXJ && (j + 2) * k <= GM_MAXOUT) {
+        // row-parallel kernels: h1 = V'W and ||W||^2; W -= V h1 with
+        // h2 = V'W and ||W||^2 of the result in the same pass; a second
+        // pass only where a norm fell below 1/sqrt(2) of its value before
+        // (the decision is a device flag the second-pass kernel reads)
+        const int J = j + 1;
+        gm_rows<T, false, true>(n, k, J, V.p, ldV, W.p, nullptr, nullptr, O1.p);
+        gm_rows<T, true, true>(n, k, J, V.p, ldV, W.p, O1.p, nullptr, O2.p);
+        k_gm_decide<T><<<1, 32, 0, stream()>>>(O1.p, O2.p, J, k, m, j, H.p, Nf.p, reorth.p);
         PB_LAUNCH_CHECK();
-        gm_mvsd<T>(n, rows, k, T(-1), V.p, ldV, D.p, rows, T(1), W.p, k);
+        gm_rows<T, true, false>(n, k, J, V.p, ldV, W.p, O2.p, reorth.p, Nf.p);
+        nrm_p = Nf.p;
+        nrm_stride = 1;
+      } else {
+        // CGS2 as block products
+        for (int pass = 0; pass < 2; pass++) {
+          launch_mvTmv<T>(n, rows, k, T(1), V.p, ldV, W.p, k, T(0), C.p, rows);
+          k_gm_extract<T><<<std::max(1, (rows * k + 255) / 256), 256, 0, stream()>>>(C.p, rows, j, k, m, H.p, D.p,
+                                                                                     pass);
+          PB_LAUNCH_CHECK();
+          gm_mvsd<T>(n, rows, k, T(-1), V.p, ldV, D.p, rows, T(1), W.p, k);
+        }
+        gram(W.p);
       }
-      gram(W.p);
-      k_gm_step<T><<<1, 32, 0, stream()>>>(Gk.p, j, k, m, H.p, cs.p, sn.p, g.p, bnorm.p, f.p, conv.p, jcount.p,
-                                           eps_abs, gt, dflags);
+      k_gm_step<T><<<1, 32, 0, stream()>>>(nrm_p, nrm_stride, j, k, m, H.p, cs.p, sn.p, g.p, bnorm.p, f.p, conv.p,
+                                           jcount.p, eps_abs, gt, dflags);
       PB_LAUNCH_CHECK();
       k_gm_scale_cols<T><<<gw, 256, 0, stream()>>>(W.p, k, V.p + (int64_t)(j + 1) * k, ldV, n, k, f.p);
       PB_LAUNCH_CHECK();
