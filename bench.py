@@ -156,6 +156,35 @@ def run_reference(args, rank, world):
     return 0
 
 
+def jada_forms(timeout=300):
+    """Time-to-solution of PHIST's unchanged subspacejada on this library
+    (phist_b200/lib/jada_run): 7-point Dirichlet Laplacian 64^3, the 10
+    smallest eigenpairs, block size 4, minBas 20, maxBas 40, tol 1e-10,
+    start block uniform[-1,1) seed 0; the plain FP64 drop-in (PHIST's
+    GMRES for the correction equations), the device-resident GMRES in FP64,
+    and FP32 correction equations on the device GMRES.  Each solve runs
+    twice in one process; the second (warm) wall time is reported."""
+    exe = os.path.join(ROOT, "phist_b200", "lib", "jada_run")
+    if not os.path.exists(exe):
+        return {"unavailable": "phist_b200/lib/jada_run is not built (phist_b200/solvers/Makefile)"}
+    common = ["LAPLACE3D-64", "numEigs=10", "blockSize=4", "minBas=20", "maxBas=40", "convTol=1e-10",
+              "which=SR", "seed=0", "reps=2"]
+    forms = {}
+    for name, extra in (("fp64_phist_gmres", []), ("fp64_device_gmres", ["devgmres=1"]),
+                        ("mixed_device_gmres", ["mixed=1", "devgmres=1"])):
+        try:
+            r = subprocess.run([exe] + common + extra, capture_output=True, text=True, timeout=timeout)
+            d = json.loads([ln for ln in r.stdout.splitlines() if ln.startswith("{")][-1])
+        except Exception as e:  # a failed form is reported, not fatal to the bench line
+            forms[name] = {"failed": str(e)[:200]}
+            continue
+        sec = d["wall"][-1]
+        forms[name] = {"seconds": round(sec, 4), "solves_per_s": round(1.0 / sec, 3),
+                       "outer_iterations": d["nIter"], "converged": d["nConv"],
+                       "max_res_explicit": max(d["resExplicit"][:10]), "launches": d["launches"]}
+    return {"workload": "subspacejada_laplace3d_64_10eigs", "n": 262144, "tol": 1e-10, "forms": forms}
+
+
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
@@ -164,6 +193,7 @@ def main():
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--nvecs", default=",".join(map(str, NVECS)))
+    ap.add_argument("--no-jada", action="store_true", help="skip the eigen-solve timings")
     args = ap.parse_args()
     nvecs = [int(t) for t in args.nvecs.split(",")]
 
@@ -313,6 +343,8 @@ def main():
     if rank == 0 and world == 1 and not args.no_cpu_baseline:
         line["cpu_baseline"] = {k: v for k, v in cpu_baseline(steps_budget_s=12.0, nvecs=nvecs).items()
                                 if k != "seconds"}
+    if rank == 0 and world == 1 and not args.no_jada:
+        line["jada"] = jada_forms()
     if rank == 0:
         print(json.dumps(line), flush=True)
     for k in nvecs:
