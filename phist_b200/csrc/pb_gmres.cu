@@ -217,68 +217,83 @@ __global__ void k_gm_invnorm(const T* __restrict__ G, int k, T* f)
   f[s] = nr > 0.0 ? (T)(1.0 / nr) : T(0);
 }
 
-// Row-parallel Gram-Schmidt kernels for J = j+1 <= GM_MAXJ basis blocks
-// and (J+1)*k <= GM_MAXOUT outputs.
-// Thread (row r, system s) with s = tid % KP (KP = k rounded up to a power
-// of two) walks rows with a grid stride.
-//   UPD:  w_s <- w_s - sum_i V(r, i*k+s) h[i*k+s]   (h on the device)
-//   DOTS: out[i*k+s] = sum_r V(r, i*k+s) w_s(r) for i < J, and
-//         out[J*k+s] = sum_r w_s(r)^2 (of w after the update, if any);
+// Row-parallel Gram-Schmidt kernels.  One warp per row of V (four rows of a
+// warp in flight together): the J*k coefficients of the row are read as
+// 32-wide coalesced chunks, lane l owning columns c = l + 32q (q < NQ).  k
+// divides 32, so every column a lane owns belongs to system s = l mod k.
+//   UPD:  w_s <- w_s - sum_i V(r, i*k+s) h[i*k+s]: each lane sums its
+//         columns, the lanes of one system are combined by a butterfly,
+//         and the new w_s is broadcast back to them
+//   DOTS: out[c] = sum_r V(r, c) w_{c mod k}(r) for c < J*k (of w after the
+//         update, from the same loads of V), and out[J*k+s] = ||w_s||^2;
 //         without DOTS only out[s] = ||w_s||^2.
 // skip (may be NULL): the kernel does nothing when *skip == 0.
-// Sums: butterfly over the lanes of one system, warps in order, then the
-// fixed-order last-block pass: bitwise reproducible.
-constexpr int GM_MAXJ = 24;
+// Sums: per lane over rows, warps in order, then the fixed-order last-block
+// pass: bitwise reproducible.
 constexpr int GM_MAXOUT = 256;  // (J+1)*k outputs at most
 
-template <class T, bool UPD, bool DOTS, int KP>
+template <class T, bool UPD, bool DOTS, int NQ>
 __global__ void __launch_bounds__(256) k_gm_rows(int64_t n, int k, int J, const T* __restrict__ V, int64_t ldV, T* W,
                                                  const T* __restrict__ h, const int* __restrict__ skip, T* part,
                                                  unsigned int* counter, T* out)
 {
   if (skip && *skip == 0) return;
-  constexpr int NA = DOTS ? GM_MAXJ + 1 : 1;
-  const int tid = threadIdx.x, s = tid % KP;
-  const int nout = DOTS ? (J + 1) * k : k;
-  T acc[NA];
+  constexpr int RU = 4;  // rows of one warp in flight together
+  const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
+  const int ncol = J * k;
+  const int s = lane % k;
+  const int nout = DOTS ? ncol + k : k;
+  T hq[NQ], acc[NQ];
 #pragma unroll
-  for (int i = 0; i < NA; i++) acc[i] = T(0);
-  if (s < k) {
-    const int64_t rstep = (int64_t)gridDim.x * (256 / KP);
-    for (int64_t r = blockIdx.x * (int64_t)(256 / KP) + tid / KP; r < n; r += rstep) {
-      const T* vr = V + r * ldV + s;
-      T w = W[r * k + s];
+  for (int q = 0; q < NQ; q++) {
+    const int c = lane + 32 * q;
+    hq[q] = (UPD && c < ncol) ? h[c] : T(0);
+    acc[q] = T(0);
+  }
+  T nacc = T(0);
+  const int64_t wstep = (int64_t)gridDim.x * 8;
+  for (int64_t r0 = blockIdx.x * (int64_t)8 + warp; r0 < n; r0 += RU * wstep) {
+    T v[RU][NQ], w[RU];
+#pragma unroll
+    for (int u = 0; u < RU; u++) {
+      const int64_t r = r0 + u * wstep;
+      const bool in = r < n;
+      const T* vr = V + (in ? r : 0) * ldV;
+#pragma unroll
+      for (int q = 0; q < NQ; q++) {
+        const int c = lane + 32 * q;
+        v[u][q] = (in && c < ncol) ? vr[c] : T(0);
+      }
+      w[u] = in ? W[r * k + s] : T(0);
+    }
+#pragma unroll
+    for (int u = 0; u < RU; u++) {
+      const int64_t r = r0 + u * wstep;
       if (UPD) {
-#pragma unroll 4
-        for (int i = 0; i < J; i++) w -= vr[(int64_t)i * k] * __ldg(h + i * k + s);
-        W[r * k + s] = w;
+        T p = T(0);
+#pragma unroll
+        for (int q = 0; q < NQ; q++) p += v[u][q] * hq[q];
+        for (int off = 16; off >= k; off >>= 1) p += __shfl_xor_sync(0xffffffffu, p, off);
+        w[u] -= p;  // every lane of system s now holds the same new w_s
+        if (lane < k && r < n) W[r * k + s] = w[u];
       }
       if (DOTS) {
 #pragma unroll
-        for (int i = 0; i < GM_MAXJ; i++)
-          if (i < J) acc[i] += vr[(int64_t)i * k] * w;
-        acc[GM_MAXJ] += w * w;
-      } else {
-        acc[0] += w * w;
+        for (int q = 0; q < NQ; q++) acc[q] += v[u][q] * w[u];
       }
+      if (lane < k) nacc += w[u] * w[u];
     }
   }
-  // lanes of one system: xor over the lane bits above log2(KP)
-#pragma unroll
-  for (int i = 0; i < NA; i++)
-#pragma unroll
-    for (int off = 16; off >= KP; off >>= 1) acc[i] += __shfl_xor_sync(0xffffffffu, acc[i], off);
   __shared__ T red[8][GM_MAXOUT];
-  const int lane = tid & 31, warp = tid >> 5;
-  if (lane < KP && s < k) {
-    if (DOTS) {
+  if (DOTS) {
 #pragma unroll
-      for (int i = 0; i < GM_MAXJ; i++)
-        if (i < J) red[warp][i * k + s] = acc[i];
-      red[warp][J * k + s] = acc[GM_MAXJ];
-    } else {
-      red[warp][s] = acc[0];
+    for (int q = 0; q < NQ; q++) {
+      const int c = lane + 32 * q;
+      if (c < ncol) red[warp][c] = acc[q];
     }
+    if (lane < k) red[warp][ncol + lane] = nacc;
+  } else if (lane < k) {
+    red[warp][lane] = nacc;
   }
   __syncthreads();
   for (int o = tid; o < nout; o += 256) {
@@ -318,21 +333,16 @@ __global__ void k_gm_decide(const T* __restrict__ O1, const T* __restrict__ O2, 
 template <class T, bool UPD, bool DOTS>
 void gm_rows(int64_t n, int k, int J, const T* V, int64_t ldV, T* W, const T* h, const int* skip, T* out)
 {
-  const int KP = k <= 1 ? 1 : k <= 2 ? 2 : k <= 4 ? 4 : k <= 8 ? 8 : k <= 16 ? 16 : 32;
-  const int rows_per_block = 256 / KP;
-  const int grid = (int)std::max<int64_t>(1, std::min<int64_t>(ceil_div(n, rows_per_block), rt().num_sms() * 4));
+  const int grid = (int)std::max<int64_t>(1, std::min<int64_t>(ceil_div(n, 32), rt().num_sms() * 8));
   const int nout = DOTS ? (J + 1) * k : k;
+  const int nq = (J * k + 31) / 32;
   T* part = (T*)rt().scratch(sizeof(T) * (size_t)grid * nout);
-#define PB_GMR(KPv)                                                                                         \
-  k_gm_rows<T, UPD, DOTS, KPv><<<grid, 256, 0, stream()>>>(n, k, J, V, ldV, W, h, skip, part, rt().counters(), out)
-  switch (KP) {
-    case 1: PB_GMR(1); break;
-    case 2: PB_GMR(2); break;
-    case 4: PB_GMR(4); break;
-    case 8: PB_GMR(8); break;
-    case 16: PB_GMR(16); break;
-    default: PB_GMR(32); break;
-  }
+#define PB_GMR(NQv) \
+  k_gm_rows<T, UPD, DOTS, NQv><<<grid, 256, 0, stream()>>>(n, k, J, V, ldV, W, h, skip, part, rt().counters(), out)
+  if (nq <= 1) PB_GMR(1);
+  else if (nq <= 2) PB_GMR(2);
+  else if (nq <= 4) PB_GMR(4);
+  else PB_GMR(8);
 #undef PB_GMR
   PB_LAUNCH_CHECK();
 }
@@ -387,7 +397,7 @@ int jada_gmres(const SparseMat<T>* A, const Mvec<T>* Q, const Mvec<T>* R, const 
   DBuf<T> Gk((size_t)k * k), f(k);
   DBuf<double> H((size_t)(m + 1) * m * k), cs((size_t)m * k), sn((size_t)m * k), g((size_t)(m + 1) * k), bnorm(k);
   DBuf<int> conv(k), jcount(k), reorth(1);
-  DBuf<T> O1((size_t)(GM_MAXJ + 1) * k), O2((size_t)(GM_MAXJ + 1) * k), Nf(k);
+  DBuf<T> O1(GM_MAXOUT), O2(GM_MAXOUT), Nf(k);
   GmIndex gi;
   GmTol gt;
   for (int s = 0; s < k; s++) {
@@ -450,7 +460,7 @@ int jada_gmres(const SparseMat<T>* A, const Mvec<T>* Q, const Mvec<T>* R, const 
       const int rows = (j + 1) * k;
       const T* nrm_p = Gk.p;
       int nrm_stride = k + 1;
-      if (j + 1 <= GM_MAXJ && (j + 2) * k <= GM_MAXOUT) {
+      if ((j + 2) * k <= GM_MAXOUT && (32 % k) == 0) {
         // row-parallel kernels: h1 = V'W and ||W||^2; W -= V h1 with
         // h2 = V'W and ||W||^2 of the result in the same pass; a second
         // pass only where a norm fell below 1/sqrt(2) of its value before
