@@ -8,13 +8,11 @@
 // orthogonalises by iterated modified Gram-Schmidt, one mvec_dot_mvec per
 // previous basis block, each a host round trip, and the Hessenberg matrix
 // and Givens rotations live on the host.  Here the k systems run as k
-// columns of one block: every basis block V_i is n x k, the Hessenberg
-// matrices, rotations and residual estimates stay on the device, and the
-// Gram-Schmidt step is classical Gram-Schmidt done twice (CGS2) as two
-// block products per pass: C = [V_0..V_j]' W on the tensor-core mvTmv
-// kernels, then W -= [V_0..V_j] D with D the block-diagonal part of C
-// (system s only uses the coefficients of its own column).  An iteration is
-// ~15 asynchronous launches with no host synchronisation; after each step
+// columns of one block: every basis block V_i is a contiguous n x k array,
+// the Hessenberg matrices, rotations and residual estimates stay on the
+// device, and the Gram-Schmidt step is classical with selective
+// reorthogonalisation in row-parallel kernels (see k_gm_blk).  An iteration
+// is ~10 asynchronous launches with no host synchronisation; after each step
 // the host looks (without waiting) at a step counter and converged count the
 // device writes into mapped host memory, and stops launching once every
 // system has converged.
@@ -111,27 +109,6 @@ __global__ void k_gm_start(const T* __restrict__ G, int k, int m, double* g, dou
   (void)tol;
 }
 
-// One CGS pass: from C = [V_0..V_j]' W (rows (j+1)k, column-major, ld ldc)
-// take h(i, s) = C(i*k + s, s) into H(i, j, s) (pass 0 sets, pass 1 adds)
-// and build D ((j+1)k x k, ld (j+1)k) with D(i*k + s, s) = h(i, s), zero
-// elsewhere.
-template <class T>
-__global__ void k_gm_extract(const T* __restrict__ C, int ldc, int j, int k, int m, double* H, T* D, int pass)
-{
-  const int rows = (j + 1) * k;
-  for (int e = blockIdx.x * blockDim.x + threadIdx.x; e < rows * k; e += gridDim.x * blockDim.x) {
-    const int r = e % rows, c = e / rows;
-    const int i = r / k, s = r - i * k;
-    T v = T(0);
-    if (s == c) {
-      v = C[r + (int64_t)c * ldc];
-      double* h = H + ((int64_t)i * m + j) * k + s;
-      *h = pass ? *h + (double)v : (double)v;
-    }
-    D[r + (int64_t)c * rows] = v;
-  }
-}
-
 // After W is orthogonal to V_0..V_j: h(j+1, j, s) = ||w_s|| (diagonal of
 // W'W), the earlier rotations applied to column j of H(:, :, s), a new
 // rotation zeroing h(j+1, j), the residual estimate |g_{j+1}| and the
@@ -186,16 +163,16 @@ __global__ void k_gm_step(const T* __restrict__ G, int gstride, int j, int k, in
   }
 }
 
-// y_s = H(0:J_s, 0:J_s, s)^{-1} g(0:J_s, s), J_s = jcount[s], into the
-// coefficient block Y (Jmax*k x k, ld Jmax*k): Y(i*k + s, s) = y_s(i).
+// y_s = H(0:J_s, 0:J_s, s)^{-1} g(0:J_s, s), J_s = jcount[s], stored
+// negated as update coefficients: Y[i*k + s] = -y_s(i) for i < J_s, 0 up to
+// Jmax (x -= sum_i V_i Y_i is then x += V y).
 template <class T>
 __global__ void k_gm_solve(const double* __restrict__ H, const double* __restrict__ g, const int* __restrict__ jcount,
                            int k, int m, int Jmax, T* Y)
 {
   const int s = threadIdx.x;
   if (s >= k) return;
-  const int rows = Jmax * k;
-  for (int r = 0; r < rows; r++) Y[r + (int64_t)s * rows] = T(0);
+  for (int i = 0; i < Jmax; i++) Y[i * k + s] = T(0);
   const int J = jcount[s];
   double y[64];
   for (int i = J - 1; i >= 0; i--) {
@@ -204,7 +181,7 @@ __global__ void k_gm_solve(const double* __restrict__ H, const double* __restric
     const double d = H[((int64_t)i * m + i) * k + s];
     y[i] = (d != 0.0) ? v / d : 0.0;
   }
-  for (int i = 0; i < J; i++) Y[(i * k + s) + (int64_t)s * rows] = (T)y[i];
+  for (int i = 0; i < J; i++) Y[i * k + s] = (T)(-y[i]);
 }
 
 // 1/||x_s|| from the diagonal of X'X (0 for a zero column)
@@ -217,91 +194,84 @@ __global__ void k_gm_invnorm(const T* __restrict__ G, int k, T* f)
   f[s] = nr > 0.0 ? (T)(1.0 / nr) : T(0);
 }
 
-// Row-parallel Gram-Schmidt kernels.  One warp per row of V (four rows of a
-// warp in flight together): the J*k coefficients of the row are read as
-// 32-wide coalesced chunks, lane l owning columns c = l + 32q (q < NQ).  k
-// divides 32, so every column a lane owns belongs to system s = l mod k.
-//   UPD:  w_s <- w_s - sum_i V(r, i*k+s) h[i*k+s]: each lane sums its
-//         columns, the lanes of one system are combined by a butterfly,
-//         and the new w_s is broadcast back to them
-//   DOTS: out[c] = sum_r V(r, c) w_{c mod k}(r) for c < J*k (of w after the
-//         update, from the same loads of V), and out[J*k+s] = ||w_s||^2;
-//         without DOTS only out[s] = ||w_s||^2.
+// Row-parallel Gram-Schmidt kernel over the basis blocks V_i, i in [i0, i1)
+// (at most MJ <= GM_MAXJ of them, held in registers), V_i = V + i*n*k, each n x k contiguous.
+// Thread (row r, system s), s = tid % KP (KP = k rounded up to a power of
+// two): a warp covers 32/KP consecutive rows, so every load of V_i or W is
+// one contiguous segment.
+//   UPD:  w_s <- w_s - sum_i V_i(r, s) h[i*k + s]
+//   DOTS: out[i*k + s] = sum_r V_i(r, s) w_s(r) (w after the update, from
+//         the same loads of V), i in [i0, i1), at out + i0*k
+//   always: ||w_s||^2 after the update, at out + i1*k (DOTS) or out (not)
 // skip (may be NULL): the kernel does nothing when *skip == 0.
-// Sums: per lane over rows, warps in order, then the fixed-order last-block
-// pass: bitwise reproducible.
-constexpr int GM_MAXOUT = 256;  // (J+1)*k outputs at most
+// Sums: butterfly over the lanes of one system, warps in order, then the
+// fixed-order last-block pass: bitwise reproducible.
+constexpr int GM_MAXJ = 16;
+constexpr int GM_MAXOUT = 256;
 
-template <class T, bool UPD, bool DOTS, int NQ>
-__global__ void __launch_bounds__(256) k_gm_rows(int64_t n, int k, int J, const T* __restrict__ V, int64_t ldV, T* W,
-                                                 const T* __restrict__ h, const int* __restrict__ skip, T* part,
-                                                 unsigned int* counter, T* out)
+template <class T, bool UPD, bool DOTS, int MJ>
+__global__ void __launch_bounds__(256) k_gm_blk(int64_t n, int k, int kp, int i0, int i1, const T* __restrict__ V,
+                                                T* W, const T* __restrict__ h, const int* __restrict__ skip, T* part,
+                                                unsigned int* counter, T* out)
 {
   if (skip && *skip == 0) return;
-  constexpr int RU = 4;  // rows of one warp in flight together
   const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
-  const int ncol = J * k;
-  const int s = lane % k;
-  const int nout = DOTS ? ncol + k : k;
-  T hq[NQ], acc[NQ];
+  const int s = tid % kp, nb = i1 - i0;
+  const int nout = (DOTS ? nb + 1 : 1) * k;
+  const int64_t nk = n * (int64_t)k;
+  T hc[MJ], acc[MJ];
 #pragma unroll
-  for (int q = 0; q < NQ; q++) {
-    const int c = lane + 32 * q;
-    hq[q] = (UPD && c < ncol) ? h[c] : T(0);
-    acc[q] = T(0);
+  for (int i = 0; i < MJ; i++) {
+    hc[i] = (UPD && i < nb && s < k) ? h[(i0 + i) * k + s] : T(0);
+    acc[i] = T(0);
   }
   T nacc = T(0);
-  const int64_t wstep = (int64_t)gridDim.x * 8;
-  for (int64_t r0 = blockIdx.x * (int64_t)8 + warp; r0 < n; r0 += RU * wstep) {
-    T v[RU][NQ], w[RU];
+  if (s < k) {
+    const int64_t rstep = (int64_t)gridDim.x * (256 / kp);
+    for (int64_t r = blockIdx.x * (int64_t)(256 / kp) + tid / kp; r < n; r += rstep) {
+      const T* vr = V + (int64_t)i0 * nk + r * k + s;
+      T v[MJ];
 #pragma unroll
-    for (int u = 0; u < RU; u++) {
-      const int64_t r = r0 + u * wstep;
-      const bool in = r < n;
-      const T* vr = V + (in ? r : 0) * ldV;
-#pragma unroll
-      for (int q = 0; q < NQ; q++) {
-        const int c = lane + 32 * q;
-        v[u][q] = (in && c < ncol) ? vr[c] : T(0);
-      }
-      w[u] = in ? W[r * k + s] : T(0);
-    }
-#pragma unroll
-    for (int u = 0; u < RU; u++) {
-      const int64_t r = r0 + u * wstep;
+      for (int i = 0; i < MJ; i++) v[i] = (i < nb) ? vr[(int64_t)i * nk] : T(0);
+      T w = W[r * k + s];
       if (UPD) {
-        T p = T(0);
 #pragma unroll
-        for (int q = 0; q < NQ; q++) p += v[u][q] * hq[q];
-        for (int off = 16; off >= k; off >>= 1) p += __shfl_xor_sync(0xffffffffu, p, off);
-        w[u] -= p;  // every lane of system s now holds the same new w_s
-        if (lane < k && r < n) W[r * k + s] = w[u];
+        for (int i = 0; i < MJ; i++) w -= v[i] * hc[i];
+        W[r * k + s] = w;
       }
       if (DOTS) {
 #pragma unroll
-        for (int q = 0; q < NQ; q++) acc[q] += v[u][q] * w[u];
+        for (int i = 0; i < MJ; i++) acc[i] += v[i] * w;
       }
-      if (lane < k) nacc += w[u] * w[u];
+      nacc += w * w;
     }
   }
-  __shared__ T red[8][GM_MAXOUT];
-  if (DOTS) {
 #pragma unroll
-    for (int q = 0; q < NQ; q++) {
-      const int c = lane + 32 * q;
-      if (c < ncol) red[warp][c] = acc[q];
+  for (int off = 16; off >= 1; off >>= 1) {
+    if (off < kp) break;
+#pragma unroll
+    for (int i = 0; i < MJ; i++)
+      if (DOTS && i < nb) acc[i] += __shfl_xor_sync(0xffffffffu, acc[i], off);
+    nacc += __shfl_xor_sync(0xffffffffu, nacc, off);
+  }
+  __shared__ T red[8][GM_MAXOUT];
+  if (lane < kp && s < k) {
+    if (DOTS) {
+#pragma unroll
+      for (int i = 0; i < MJ; i++)
+        if (i < nb) red[warp][i * k + s] = acc[i];
+      red[warp][nb * k + s] = nacc;
+    } else {
+      red[warp][s] = nacc;
     }
-    if (lane < k) red[warp][ncol + lane] = nacc;
-  } else if (lane < k) {
-    red[warp][lane] = nacc;
   }
   __syncthreads();
   for (int o = tid; o < nout; o += 256) {
-    T v = T(0);
-    for (int w8 = 0; w8 < 8; w8++) v += red[w8][o];
-    part[(int64_t)blockIdx.x * nout + o] = v;
+    T a = T(0);
+    for (int w8 = 0; w8 < 8; w8++) a += red[w8][o];
+    part[(int64_t)blockIdx.x * nout + o] = a;
   }
-  last_block_reduce<T>(part, nout, gridDim.x, counter, out, 1, nout, 0, T(1), T(0));
+  last_block_reduce<T>(part, nout, gridDim.x, counter, out + (DOTS ? (int64_t)i0 * k : 0), 1, nout, 0, T(1), T(0));
 }
 
 // After pass 1: O1 = (h1, ||w||^2 before), O2 = (h2, ||w||^2 after).  H(:, j)
@@ -330,21 +300,44 @@ __global__ void k_gm_decide(const T* __restrict__ O1, const T* __restrict__ O2, 
   if (s == 0) *reorth = any;
 }
 
+// Blocks per launch of k_gm_blk for k systems
+inline int gm_chunk(int k) { return std::max(1, std::min(GM_MAXJ, GM_MAXOUT / k - 1)); }
+
+// one launch of k_gm_blk over the blocks [i0, i1)
 template <class T, bool UPD, bool DOTS>
-void gm_rows(int64_t n, int k, int J, const T* V, int64_t ldV, T* W, const T* h, const int* skip, T* out)
+void gm_blk(int64_t n, int k, int i0, int i1, const T* V, T* W, const T* h, const int* skip, T* out)
 {
-  const int grid = (int)std::max<int64_t>(1, std::min<int64_t>(ceil_div(n, 32), rt().num_sms() * 8));
-  const int nout = DOTS ? (J + 1) * k : k;
-  const int nq = (J * k + 31) / 32;
+  const int kp = k <= 1 ? 1 : k <= 2 ? 2 : k <= 4 ? 4 : k <= 8 ? 8 : k <= 16 ? 16 : 32;
+  const int grid = (int)std::max<int64_t>(1, std::min<int64_t>(ceil_div(n, 256 / kp), rt().num_sms() * 8));
+  const int nout = (DOTS ? i1 - i0 + 1 : 1) * k;
   T* part = (T*)rt().scratch(sizeof(T) * (size_t)grid * nout);
-#define PB_GMR(NQv) \
-  k_gm_rows<T, UPD, DOTS, NQv><<<grid, 256, 0, stream()>>>(n, k, J, V, ldV, W, h, skip, part, rt().counters(), out)
-  if (nq <= 1) PB_GMR(1);
-  else if (nq <= 2) PB_GMR(2);
-  else if (nq <= 4) PB_GMR(4);
-  else PB_GMR(8);
-#undef PB_GMR
+  // the fewest register-held blocks that cover this launch
+  const int nb = i1 - i0;
+#define PB_GMB(MJv) \
+  k_gm_blk<T, UPD, DOTS, MJv><<<grid, 256, 0, stream()>>>(n, k, kp, i0, i1, V, W, h, skip, part, rt().counters(), out)
+  if (nb <= 4) PB_GMB(4);
+  else if (nb <= 8) PB_GMB(8);
+  else PB_GMB(16);
+#undef PB_GMB
   PB_LAUNCH_CHECK();
+}
+
+// out[i*k + s] = V_i' w_s for i < J and out[J*k + s] = ||w_s||^2, over
+// chunks of blocks in ascending order (a chunk's norm lands where the next
+// chunk's dots go and is overwritten by them; the last one stays)
+template <class T>
+void gm_dots(int64_t n, int k, int J, const T* V, T* W, T* out)
+{
+  const int cj = gm_chunk(k);
+  for (int i0 = 0; i0 < J; i0 += cj) gm_blk<T, false, true>(n, k, i0, std::min(J, i0 + cj), V, W, nullptr, nullptr, out);
+}
+
+// w -= sum_{i<J} V_i h_i; ||w||^2 into nrm
+template <class T>
+void gm_update(int64_t n, int k, int J, const T* V, T* W, const T* h, const int* skip, T* nrm)
+{
+  const int cj = gm_chunk(k);
+  for (int i0 = 0; i0 < J; i0 += cj) gm_blk<T, true, false>(n, k, i0, std::min(J, i0 + cj), V, W, h, skip, nrm);
 }
 
 }  // namespace
@@ -389,15 +382,15 @@ int jada_gmres(const SparseMat<T>* A, const Mvec<T>* Q, const Mvec<T>* R, const 
   }
   const int nq = Q ? Q->nvec : 0;
   const int m = std::max(1, std::min(std::min(maxBas > 0 ? maxBas : maxIter, maxIter), 63));
-  const int64_t ldV = (int64_t)(m + 1) * k;
+  const int64_t nk = n * (int64_t)k;  // one basis block
   const double eps_abs = 1000.0 * std::numeric_limits<T>::epsilon();
 
-  DBuf<T> V((size_t)n * ldV), B((size_t)n * k), X((size_t)n * k), W((size_t)n * k);
-  DBuf<T> C((size_t)(m + 1) * k * k), D((size_t)(m + 1) * k * k), Cq((size_t)std::max(nq, 1) * k);
+  DBuf<T> V((size_t)nk * (m + 1)), B((size_t)nk), X((size_t)nk), W((size_t)nk);
+  DBuf<T> Y((size_t)(m + 1) * k), Cq((size_t)std::max(nq, 1) * k), dummy(k);
   DBuf<T> Gk((size_t)k * k), f(k);
   DBuf<double> H((size_t)(m + 1) * m * k), cs((size_t)m * k), sn((size_t)m * k), g((size_t)(m + 1) * k), bnorm(k);
   DBuf<int> conv(k), jcount(k), reorth(1);
-  DBuf<T> O1(GM_MAXOUT), O2(GM_MAXOUT), Nf(k);
+  DBuf<T> O1((size_t)(m + 2) * k), O2((size_t)(m + 2) * k), Nf(k);
   GmIndex gi;
   GmTol gt;
   for (int s = 0; s < k; s++) {
@@ -444,7 +437,7 @@ int jada_gmres(const SparseMat<T>* A, const Mvec<T>* Q, const Mvec<T>* R, const 
     k_gm_start<T><<<1, 32, 0, stream()>>>(Gk.p, k, m, g.p, bnorm.p, f.p, conv.p, jcount.p, cycle == 0 ? 1 : 0,
                                           eps_abs, gt);
     PB_LAUNCH_CHECK();
-    k_gm_scale_cols<T><<<gw, 256, 0, stream()>>>(W.p, k, V.p, ldV, n, k, f.p);
+    k_gm_scale_cols<T><<<gw, 256, 0, stream()>>>(W.p, k, V.p, k, n, k, f.p);
     PB_LAUNCH_CHECK();
     hflags[1] = 0;
     hflags[0] = -1;
@@ -453,41 +446,32 @@ int jada_gmres(const SparseMat<T>* A, const Mvec<T>* Q, const Mvec<T>* R, const 
     bool stop = false;
     for (j = 0; j < jmax && !stop; j++) {
       // W = P (A - sigma I) V_j
-      raw_view(mVj, V.p + (int64_t)j * k, n, k, ldV);
+      raw_view(mVj, V.p + (int64_t)j * nk, n, k, k);
       spmv_general<T>(T(1), A, negsig.data(), &mVj, T(0), &mW, nullptr, nullptr, T(0), T(0), nullptr);
       project();
-      // Gram-Schmidt against V_0..V_j
-      const int rows = (j + 1) * k;
-      const T* nrm_p = Gk.p;
-      int nrm_stride = k + 1;
-      if ((j + 2) * k <= GM_MAXOUT && (32 % k) == 0) {
-        // row-parallel kernels: h1 = V'W and ||W||^2; W -= V h1 with
-        // h2 = V'W and ||W||^2 of the result in the same pass; a second
-        // pass only where a norm fell below 1/sqrt(2) of its value before
-        // (the decision is a device flag the second-pass kernel reads)
-        const int J = j + 1;
-        gm_rows<T, false, true>(n, k, J, V.p, ldV, W.p, nullptr, nullptr, O1.p);
-        gm_rows<T, true, true>(n, k, J, V.p, ldV, W.p, O1.p, nullptr, O2.p);
-        k_gm_decide<T><<<1, 32, 0, stream()>>>(O1.p, O2.p, J, k, m, j, H.p, Nf.p, reorth.p);
-        PB_LAUNCH_CHECK();
-        gm_rows<T, true, false>(n, k, J, V.p, ldV, W.p, O2.p, reorth.p, Nf.p);
-        nrm_p = Nf.p;
-        nrm_stride = 1;
+      // Gram-Schmidt against V_0..V_j: h1 = V'W and ||W||^2; W -= V h1,
+      // then h2 = V'W and ||W||^2 of the result (in one pass while the
+      // blocks fit one launch); a second subtraction only where a norm fell
+      // below 1/sqrt(2) of its value before (a device flag the second-pass
+      // kernels read)
+      const int J = j + 1;
+      if (J <= gm_chunk(k)) {
+        gm_blk<T, false, true>(n, k, 0, J, V.p, W.p, nullptr, nullptr, O1.p);
+        gm_blk<T, true, true>(n, k, 0, J, V.p, W.p, O1.p, nullptr, O2.p);
       } else {
-        // CGS2 as block products
-        for (int pass = 0; pass < 2; pass++) {
-          launch_mvTmv<T>(n, rows, k, T(1), V.p, ldV, W.p, k, T(0), C.p, rows);
-          k_gm_extract<T><<<std::max(1, (rows * k + 255) / 256), 256, 0, stream()>>>(C.p, rows, j, k, m, H.p, D.p,
-                                                                                     pass);
-          PB_LAUNCH_CHECK();
-          gm_mvsd<T>(n, rows, k, T(-1), V.p, ldV, D.p, rows, T(1), W.p, k);
-        }
-        gram(W.p);
+        gm_dots<T>(n, k, J, V.p, W.p, O1.p);
+        gm_update<T>(n, k, J, V.p, W.p, O1.p, nullptr, dummy.p);
+        gm_dots<T>(n, k, J, V.p, W.p, O2.p);
       }
+      k_gm_decide<T><<<1, 32, 0, stream()>>>(O1.p, O2.p, J, k, m, j, H.p, Nf.p, reorth.p);
+      PB_LAUNCH_CHECK();
+      gm_update<T>(n, k, J, V.p, W.p, O2.p, reorth.p, Nf.p);
+      const T* nrm_p = Nf.p;
+      const int nrm_stride = 1;
       k_gm_step<T><<<1, 32, 0, stream()>>>(nrm_p, nrm_stride, j, k, m, H.p, cs.p, sn.p, g.p, bnorm.p, f.p, conv.p,
                                            jcount.p, eps_abs, gt, dflags);
       PB_LAUNCH_CHECK();
-      k_gm_scale_cols<T><<<gw, 256, 0, stream()>>>(W.p, k, V.p + (int64_t)(j + 1) * k, ldV, n, k, f.p);
+      k_gm_scale_cols<T><<<gw, 256, 0, stream()>>>(W.p, k, V.p + (int64_t)(j + 1) * nk, k, n, k, f.p);
       PB_LAUNCH_CHECK();
       steps = j + 1;
       // stop launching once the device reports every system converged (a
@@ -500,9 +484,9 @@ int jada_gmres(const SparseMat<T>* A, const Mvec<T>* Q, const Mvec<T>* R, const 
     rt().sync();
     nconv = hflags[1];
     const int J = steps;
-    k_gm_solve<T><<<1, 32, 0, stream()>>>(H.p, g.p, jcount.p, k, m, J, D.p);
+    k_gm_solve<T><<<1, 32, 0, stream()>>>(H.p, g.p, jcount.p, k, m, J, Y.p);
     PB_LAUNCH_CHECK();
-    gm_mvsd<T>(n, J * k, k, T(1), V.p, ldV, D.p, J * k, T(1), X.p, k);
+    gm_update<T>(n, k, J, V.p, X.p, Y.p, nullptr, dummy.p);
   }
   // t = x / ||x||, column by column
   gram(X.p);

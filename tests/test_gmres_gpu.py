@@ -54,7 +54,9 @@ def _run(rp, c, v, Q, R, sigma, tol, max_iter, max_bas, res_index=None, dtype=np
 @pytest.mark.parametrize("problem,nq,k,max_iter,max_bas", [("LAPDIAG3D-8-S1", 6, 4, 7, 20),
                                                            ("LAPDIAG3D-8-S1", 6, 4, 12, 4),
                                                            ("HONEYCOMB-12-S3-W1", 3, 2, 9, 5),
-                                                           ("LAPLACE3D-7", 0, 3, 10, 20)])
+                                                           ("LAPLACE3D-7", 0, 3, 10, 20),
+                                                           ("LAPDIAG3D-9-S4", 4, 4, 30, 30),
+                                                           ("LAPDIAG3D-8-S1", 2, 8, 22, 22)])
 def test_gmres_cut_off_matches_oracle(session, oracle, problem, nq, k, max_iter, max_bas):
     """no convergence within max_iter (tolerance unreachable): the iterate of
     exactly max_iter steps, with restarts every max_bas steps"""
