@@ -212,7 +212,7 @@ constexpr int GM_MAXOUT = 256;
 template <class T, bool UPD, bool DOTS, int MJ>
 __global__ void __launch_bounds__(256) k_gm_blk(int64_t n, int k, int kp, int i0, int i1, const T* __restrict__ V,
                                                 T* W, const T* __restrict__ h, const int* __restrict__ skip, T* part,
-                                                unsigned int* counter, T* out)
+                                                unsigned int* counter, T* out, int ext)
 {
   if (skip && *skip == 0) return;
   const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
@@ -271,6 +271,7 @@ __global__ void __launch_bounds__(256) k_gm_blk(int64_t n, int k, int kp, int i0
     for (int w8 = 0; w8 < 8; w8++) a += red[w8][o];
     part[(int64_t)blockIdx.x * nout + o] = a;
   }
+  if (ext) return;  // second pass: k_reduce_partials
   last_block_reduce<T>(part, nout, gridDim.x, counter, out + (DOTS ? (int64_t)i0 * k : 0), 1, nout, 0, T(1), T(0));
 }
 
@@ -300,6 +301,16 @@ __global__ void k_gm_decide(const T* __restrict__ O1, const T* __restrict__ O2, 
   if (s == 0) *reorth = any;
 }
 
+// out[o] = sum over blocks of part[b*nout + o] (k_reduce_partials) unless
+// *skip == 0
+template <class T>
+__global__ void __launch_bounds__(256) k_gm_reduce_if(const T* __restrict__ part, int nblocks, int nout, T* out,
+                                                      const int* __restrict__ skip)
+{
+  if (skip && *skip == 0) return;
+  k_reduce_partials_body<T>(part, nblocks, nout, out, nout, 0, T(1), T(0));
+}
+
 // Blocks per launch of k_gm_blk for k systems
 inline int gm_chunk(int k) { return std::max(1, std::min(GM_MAXJ, GM_MAXOUT / k - 1)); }
 
@@ -308,18 +319,33 @@ template <class T, bool UPD, bool DOTS>
 void gm_blk(int64_t n, int k, int i0, int i1, const T* V, T* W, const T* h, const int* skip, T* out)
 {
   const int kp = k <= 1 ? 1 : k <= 2 ? 2 : k <= 4 ? 4 : k <= 8 ? 8 : k <= 16 ? 16 : 32;
-  const int grid = (int)std::max<int64_t>(1, std::min<int64_t>(ceil_div(n, 256 / kp), rt().num_sms() * 8));
   const int nout = (DOTS ? i1 - i0 + 1 : 1) * k;
-  T* part = (T*)rt().scratch(sizeof(T) * (size_t)grid * nout);
-  // the fewest register-held blocks that cover this launch
+  T* dst = out + (DOTS ? (int64_t)i0 * k : 0);
+  // the fewest register-held blocks that cover this launch; one wave of
+  // resident blocks, each thread walking several rows, so that few partial
+  // sums are left; many partials go to the GPU-wide second pass
   const int nb = i1 - i0;
-#define PB_GMB(MJv) \
-  k_gm_blk<T, UPD, DOTS, MJv><<<grid, 256, 0, stream()>>>(n, k, kp, i0, i1, V, W, h, skip, part, rt().counters(), out)
-  if (nb <= 4) PB_GMB(4);
-  else if (nb <= 8) PB_GMB(8);
-  else PB_GMB(16);
-#undef PB_GMB
-  PB_LAUNCH_CHECK();
+  auto launch = [&](auto kern) {
+    static int occ = 0;  // resident blocks per SM of this instantiation
+    if (occ == 0) {
+      int b = 0;
+      PB_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&b, kern, 256, 0));
+      occ = std::max(1, b);
+    }
+    const int grid = (int)std::max<int64_t>(1, std::min<int64_t>(ceil_div(n, 256 / kp), (int64_t)rt().num_sms() * occ));
+    const int ext = (nout >= 32 && grid > 32) ? 1 : 0;
+    T* part = (T*)rt().scratch(sizeof(T) * (size_t)grid * nout);
+    kern<<<grid, 256, 0, stream()>>>(n, k, kp, i0, i1, V, W, h, skip, part, rt().counters(), out, ext);
+    PB_LAUNCH_CHECK();
+    if (ext) {
+      // skipped passes leave their partials unread: k_gm_reduce_if checks the flag too
+      k_gm_reduce_if<T><<<(nout + 31) / 32, 256, 0, stream()>>>(part, grid, nout, dst, skip);
+      PB_LAUNCH_CHECK();
+    }
+  };
+  if (nb <= 4) launch(k_gm_blk<T, UPD, DOTS, 4>);
+  else if (nb <= 8) launch(k_gm_blk<T, UPD, DOTS, 8>);
+  else launch(k_gm_blk<T, UPD, DOTS, 16>);
 }
 
 // out[i*k + s] = V_i' w_s for i < J and out[J*k + s] = ||w_s||^2, over

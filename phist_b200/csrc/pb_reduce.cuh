@@ -132,8 +132,8 @@ namespace pb {
 //   out(i, j) = alpha * sum_b part[b*nout + o] + beta * out(i, j),
 //   o = i + j*mrows, out(i, j) at C[i + j*ldc]
 template <class T>
-__global__ void __launch_bounds__(256) k_reduce_partials(const T* __restrict__ part, int nblocks, int nout,
-                                                         T* C, int mrows, int64_t ldc, T alpha, T beta)
+__device__ __forceinline__ void k_reduce_partials_body(const T* __restrict__ part, int nblocks, int nout, T* C,
+                                                       int mrows, int64_t ldc, T alpha, T beta)
 {
   __shared__ T red[8][32];
   const int ol = threadIdx.x & 31, ch = threadIdx.x >> 5;
@@ -163,6 +163,13 @@ __global__ void __launch_bounds__(256) k_reduce_partials(const T* __restrict__ p
     T* dst = C + (o % mrows) + (int64_t)(o / mrows) * ldc;
     *dst = (beta == T(0)) ? alpha * t : alpha * t + beta * *dst;
   }
+}
+
+template <class T>
+__global__ void __launch_bounds__(256) k_reduce_partials(const T* __restrict__ part, int nblocks, int nout,
+                                                         T* C, int mrows, int64_t ldc, T alpha, T beta)
+{
+  k_reduce_partials_body<T>(part, nblocks, nout, C, mrows, ldc, alpha, beta);
 }
 
 }  // namespace pb
