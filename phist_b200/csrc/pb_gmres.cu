@@ -127,13 +127,21 @@ __global__ void k_gm_step(const T* __restrict__ G, int gstride, int j, int k, in
   if (s < k) {
     const double hn = sqrt(fmax((double)G[s * gstride], 0.0));
     auto Hat = [&](int i) -> double& { return H[((int64_t)i * m + j) * k + s]; };
+    // column j of H and the earlier rotations, all loads issued before the
+    // dependent chain of rotations
+    double hc[64], rc[64], rs[64];
+    for (int i = 0; i <= j; i++) hc[i] = Hat(i);
     for (int i = 0; i < j; i++) {
-      const double a = Hat(i), b = Hat(i + 1);
-      const double c = cs[i * k + s], sn_ = sn[i * k + s];
-      Hat(i) = c * a + sn_ * b;
-      Hat(i + 1) = -sn_ * a + c * b;
+      rc[i] = cs[i * k + s];
+      rs[i] = sn[i * k + s];
     }
-    const double a = Hat(j);
+    for (int i = 0; i < j; i++) {
+      const double a = hc[i], b = hc[i + 1];
+      hc[i] = rc[i] * a + rs[i] * b;
+      hc[i + 1] = -rs[i] * a + rc[i] * b;
+    }
+    for (int i = 0; i < j; i++) Hat(i) = hc[i];
+    const double a = hc[j];
     double c = 1.0, sn_ = 0.0;
     const double r = hypot(a, hn);
     if (r > 0.0) {
