@@ -319,6 +319,20 @@ __global__ void __launch_bounds__(256) k_gm_reduce_if(const T* __restrict__ part
   k_reduce_partials_body<T>(part, nblocks, nout, out, nout, 0, T(1), T(0));
 }
 
+// resident 256-thread blocks per SM of one k_gm_blk instantiation (queried
+// once)
+template <class T, bool UPD, bool DOTS, int MJ>
+int gm_occ()
+{
+  static int occ = 0;
+  if (occ == 0) {
+    int b = 0;
+    PB_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&b, k_gm_blk<T, UPD, DOTS, MJ>, 256, 0));
+    occ = std::max(1, b);
+  }
+  return occ;
+}
+
 // Blocks per launch of k_gm_blk for k systems
 inline int gm_chunk(int k) { return std::max(1, std::min(GM_MAXJ, GM_MAXOUT / k - 1)); }
 
@@ -333,13 +347,7 @@ void gm_blk(int64_t n, int k, int i0, int i1, const T* V, T* W, const T* h, cons
   // resident blocks, each thread walking several rows, so that few partial
   // sums are left; many partials go to the GPU-wide second pass
   const int nb = i1 - i0;
-  auto launch = [&](auto kern) {
-    static int occ = 0;  // resident blocks per SM of this instantiation
-    if (occ == 0) {
-      int b = 0;
-      PB_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&b, kern, 256, 0));
-      occ = std::max(1, b);
-    }
+  auto launch = [&](auto kern, int occ) {
     const int grid = (int)std::max<int64_t>(1, std::min<int64_t>(ceil_div(n, 256 / kp), (int64_t)rt().num_sms() * occ));
     const int ext = (nout >= 32 && grid > 32) ? 1 : 0;
     T* part = (T*)rt().scratch(sizeof(T) * (size_t)grid * nout);
@@ -351,9 +359,9 @@ void gm_blk(int64_t n, int k, int i0, int i1, const T* V, T* W, const T* h, cons
       PB_LAUNCH_CHECK();
     }
   };
-  if (nb <= 4) launch(k_gm_blk<T, UPD, DOTS, 4>);
-  else if (nb <= 8) launch(k_gm_blk<T, UPD, DOTS, 8>);
-  else launch(k_gm_blk<T, UPD, DOTS, 16>);
+  if (nb <= 4) launch(k_gm_blk<T, UPD, DOTS, 4>, gm_occ<T, UPD, DOTS, 4>());
+  else if (nb <= 8) launch(k_gm_blk<T, UPD, DOTS, 8>, gm_occ<T, UPD, DOTS, 8>());
+  else launch(k_gm_blk<T, UPD, DOTS, 16>, gm_occ<T, UPD, DOTS, 16>());
 }
 
 // out[i*k + s] = V_i' w_s for i < J and out[J*k + s] = ||w_s||^2, over
