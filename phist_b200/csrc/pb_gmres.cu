@@ -25,6 +25,7 @@
 // unit norm (phist_jadaCorrectionSolver_def.hpp:576-578).  The small dense
 // part (Hessenberg, rotations, triangular solve) is FP64 in both precisions.
 #include <algorithm>
+#include <atomic>
 #include <cmath>
 #include <limits>
 #include <vector>
@@ -324,13 +325,15 @@ __global__ void __launch_bounds__(256) k_gm_reduce_if(const T* __restrict__ part
 template <class T, bool UPD, bool DOTS, int MJ>
 int gm_occ()
 {
-  static int occ = 0;
-  if (occ == 0) {
+  static std::atomic<int> occ{0};  // lanes on several threads may ask at once
+  int o = occ.load(std::memory_order_relaxed);
+  if (o == 0) {
     int b = 0;
     PB_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&b, k_gm_blk<T, UPD, DOTS, MJ>, 256, 0));
-    occ = std::max(1, b);
+    o = std::max(1, b);
+    occ.store(o, std::memory_order_relaxed);
   }
-  return occ;
+  return o;
 }
 
 // Blocks per launch of k_gm_blk for k systems
