@@ -140,6 +140,18 @@ def cpu_baseline(steps_budget_s=12.0, nvecs=NVECS):
             "seconds": round(total_t, 3)}
 
 
+def max_over_ranks(x, dist=None, device="cuda"):
+    """The largest of the ranks' values of x (every rank gets it): the
+    timing rule of the multi-replica runs, where the job takes as long as
+    its slowest rank.  x itself without a process group."""
+    if dist is None:
+        return x
+    import torch
+    t = torch.tensor([x], device=device, dtype=torch.float64)
+    dist.all_reduce(t, op=dist.ReduceOp.MAX)
+    return float(t.item())
+
+
 def run_reference(args, rank, world):
     if rank != 0:
         return 0
@@ -264,9 +276,7 @@ def main():
         per[k] += e0.elapsed_time(e1) * 1e-3
     dev_time = sum(per.values())
     if dist is not None:
-        t = torch.tensor([dev_time], device="cuda", dtype=torch.float64)
-        dist.all_reduce(t, op=dist.ReduceOp.MAX)
-        dev_time = float(t.item())
+        dev_time = max_over_ranks(dev_time, dist)
         dist.barrier()
     step_bytes = sum(spmv_bytes(n, nnz, k) for k in nvecs)
     value = world * step_bytes * args.steps / dev_time / 1e9
@@ -299,10 +309,7 @@ def main():
     e1.record(lib_stream)
     torch.cuda.synchronize()
     e2e_time = e0.elapsed_time(e1) * 1e-3
-    if dist is not None:
-        t = torch.tensor([e2e_time], device="cuda", dtype=torch.float64)
-        dist.all_reduce(t, op=dist.ReduceOp.MAX)
-        e2e_time = float(t.item())
+    e2e_time = max_over_ranks(e2e_time, dist)
     e2e_val = world * step_bytes * args.steps / e2e_time / 1e9
     ok = np.isfinite(hy[nvecs[-1]].numpy()).all()
 
