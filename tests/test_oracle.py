@@ -244,3 +244,38 @@ def test_oracle_jada_gmres_is_the_krylov_minimiser():
         y = P @ (A - sg * np.eye(n)) @ t[:, s]
         a = (y @ R[:, s]) / (y @ y)
         assert np.linalg.norm(a * y - R[:, s]) < 1e-9 * np.linalg.norm(R[:, s])
+
+
+def test_oracle_jada_gmres_restart_semantics():
+    """restarted GMRES(m) in the restatement: two cycles of m steps equal
+    x1 = argmin over K_m(b), then x2 = x1 + argmin over K_m(b - op x1)
+    (dense least squares on orthonormal Krylov bases), scaled to unit norm"""
+    from oracle import oracle as O
+    rng = np.random.default_rng(1)
+    n, m = 50, 4
+    A = rng.standard_normal((n, n))
+    A = A + A.T + 8 * np.eye(n)
+    Q = np.linalg.qr(rng.standard_normal((n, 2)))[0]
+    b = rng.standard_normal(n)
+    b -= Q @ (Q.T @ b)
+    sigma = 0.7
+    P = np.eye(n) - Q @ Q.T
+    op = P @ (A - sigma * np.eye(n))
+
+    def krylov_min(r):
+        K = np.zeros((n, m))
+        v = r / np.linalg.norm(r)
+        for i in range(m):
+            K[:, i] = v
+            v = op @ v
+            for _ in range(2):
+                v -= K[:, :i + 1] @ (K[:, :i + 1].T @ v)
+            v /= np.linalg.norm(v)
+        c, *_ = np.linalg.lstsq(op @ K, r, rcond=None)
+        return K @ c
+
+    x1 = krylov_min(b)
+    x2 = x1 + krylov_min(b - op @ x1)
+    t, conv = O.jada_gmres(A, Q, b[:, None], [sigma], [1e-30], 2 * m, m)
+    assert not conv[0]
+    assert np.linalg.norm(t[:, 0] - x2 / np.linalg.norm(x2)) < 1e-10
