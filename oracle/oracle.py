@@ -348,3 +348,34 @@ def jada_gmres(A, Q, R, sigma, tol, max_iter, max_bas, res_index=None):
         T[:, s] = x / nx if nx > 0 else 0.0
         conv[s] = done
     return T, conv
+
+
+def carp_cgmn(rowptr, col, val, sigma, b, iters, order=None):
+    """CGMN (CARP-CG) for the shifted systems (A - sigma_j I) x_j = b_j, one
+    per column, restated from PHIST's carp_cg
+    (src/krylov/phist_carp_cg_def.hpp:440-690): CG on (I - Q) x = Q(0, b),
+    Q(x, b) the forward-backward Kaczmarz sweep over `order` with relaxation
+    1, x_0 = 0, `iters` iterations; per column
+        r = Q(0, b), p = r
+        q = p - Q(p, 0), alpha = r'r / p'q, x += alpha p, r -= alpha q,
+        beta = r'r_new / r'r, p = r + beta p.
+    Returns x (n x nsys)."""
+    b = np.ascontiguousarray(b, np.float64)
+    n, w = b.shape
+    sig = np.asarray(sigma, np.float64)
+    om = np.ones(w)
+    x = np.zeros((n, w))
+    r = carp_sweep(rowptr, col, val, sig, b, np.zeros((n, w)), om, order)
+    p = r.copy()
+    rr = (r * r).sum(axis=0)
+    for _ in range(iters):
+        q = p - carp_sweep(rowptr, col, val, sig, None, p.copy(), om, order)
+        pq = (p * q).sum(axis=0)
+        alpha = np.where(pq != 0, rr / np.where(pq != 0, pq, 1.0), 0.0)
+        x += alpha * p
+        r -= alpha * q
+        rr_new = (r * r).sum(axis=0)
+        beta = np.where(rr != 0, rr_new / np.where(rr != 0, rr, 1.0), 0.0)
+        p = r + beta * p
+        rr = rr_new
+    return x

@@ -122,3 +122,40 @@ def test_block_tuner_and_auto_block(session, mixed):
     assert f0 == f1 == 0
     np.testing.assert_array_equal(it0, it1)
     np.testing.assert_array_equal(x0, x1)
+
+
+def test_batch_iterates_match_oracle_cgmn(session, oracle):
+    """iterate-level parity: after exactly 25 CGMN iterations (all systems in
+    slots at once, cap reached, nothing refilled) the batched solver's
+    iterates equal the numpy restatement of PHIST's recurrence
+    (oracle.carp_cgmn) over the same colour order"""
+    import ctypes as ct
+
+    from conftest import relerr
+    from phist_b200 import generators as G
+    from phist_b200 import kernels as K
+    from phist_b200.objects import Mvec, SparseMat
+    from test_carp_gpu import _order
+    rp, c, v = G.problem("HONEYCOMB-10-S3-W1")
+    n = len(rp) - 1
+    A = SparseMat.from_crs(rp, c, v)
+    sig = np.array([-4.0, 4.2, -3.8, 4.6])
+    nsys, iters = len(sig), 25
+    b = G.random_block(n, nsys, 9)
+    work = ct.c_void_p()
+    one = np.zeros(1)
+    K.chk(K.phist_Dcarp_setup, A.h, 1, K.sptr(one, np.float64), ct.byref(work))
+    rows, _ = _order(work, n)
+    K.chk(K.phist_Dcarp_destroy, A.h, work)
+    B = Mvec(A.row_map, nsys).set(b)
+    X = Mvec(A.row_map, nsys)
+    it = np.zeros(nsys, np.int32)
+    rel = np.zeros(nsys)
+    iflag = K.iflag_of(K.phist_b200_DcarpCG_batch, A.h, nsys, K.ptr(sig), B.h, X.h, nsys, 1e-30, iters, iters, 0,
+                       1e-5, K.ptr(it), K.ptr(rel))
+    x = X.get()
+    for o in (B, X, A):
+        o.delete()
+    assert iflag == nsys and (it == iters).all()
+    ref = oracle.carp_cgmn(rp, c, v, sig, b, iters, order=rows)
+    assert relerr(x, ref) < 1e-10, relerr(x, ref)

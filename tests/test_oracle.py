@@ -279,3 +279,20 @@ def test_oracle_jada_gmres_restart_semantics():
     t, conv = O.jada_gmres(A, Q, b[:, None], [sigma], [1e-30], 2 * m, m)
     assert not conv[0]
     assert np.linalg.norm(t[:, 0] - x2 / np.linalg.norm(x2)) < 1e-10
+
+
+def test_oracle_carp_cgmn_solves_shifted_systems():
+    """the CGMN restatement converges to the dense solutions of
+    (A - sigma_j I) x_j = b_j (small honeycomb, shifts outside the spectrum)"""
+    from oracle import oracle as O
+    from phist_b200 import generators as G
+    rp, c, v = G.honeycomb(6, 6, 2)
+    n = len(rp) - 1
+    A = np.zeros((n, n))
+    np.add.at(A, (np.repeat(np.arange(n), np.diff(rp)), c), v)
+    sig = np.array([-4.0, 4.5])
+    b = np.random.default_rng(0).uniform(-1, 1, (n, 2))
+    x = O.carp_cgmn(rp, c, v, sig, b, 60)
+    for j in range(2):
+        xs = np.linalg.solve(A - sig[j] * np.eye(n), b[:, j])
+        assert np.linalg.norm(x[:, j] - xs) / np.linalg.norm(xs) < 1e-10
