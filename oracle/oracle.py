@@ -22,11 +22,12 @@ REF_PREC = os.path.join(HERE, "_ref", "libref_builtin_prec.so")
 
 
 def build(with_ref=None):
-    """make -C oracle [ref]; ref only when the PHIST sources are reachable"""
+    """make -C oracle [ref]; ref only when the PHIST source tree named by
+    the PHIST_SRC environment variable is reachable"""
     targets = ["all"]
-    src = os.environ.get("PHIST_SRC", "/root/reference")
+    src = os.environ.get("PHIST_SRC", "")
     if with_ref is None:
-        with_ref = os.path.isdir(os.path.join(src, "src", "kernels", "builtin"))
+        with_ref = bool(src) and os.path.isdir(os.path.join(src, "src", "kernels", "builtin"))
     if with_ref:
         targets.append("ref")
     env = dict(os.environ, PHIST_SRC=src)

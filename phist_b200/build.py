@@ -10,7 +10,8 @@ Object files are rebuilt only when a source or header is newer.
 build_solvers() then compiles PHIST's unchanged solver layers against that
 library, together with this package's FP32 correction solver and the drivers
 (phist_b200/solvers/Makefile), when the PHIST sources are reachable
-(PHIST_SRC); without them the prebuilt outputs in phist_b200/lib are used.
+(the PHIST_SRC environment variable names the PHIST source tree); without
+them the prebuilt outputs in phist_b200/lib are used.
 """
 import os
 import subprocess
@@ -77,15 +78,37 @@ def build(verbose=False):
     return LIBPATH
 
 
+def openblas_path():
+    """The LAPACK/BLAS the solver layers link: $OPENBLAS, else the OpenBLAS
+    that the installed scipy bundles (exports LAPACKE_* and BLAS under the
+    scipy_ prefix, 32-bit integers)"""
+    env = os.environ.get("OPENBLAS")
+    if env:
+        return env
+    try:
+        import glob
+
+        import scipy
+        libs = os.path.join(os.path.dirname(os.path.dirname(scipy.__file__)), "scipy.libs")
+        cand = sorted(glob.glob(os.path.join(libs, "libscipy_openblas*.so")))
+        return cand[0] if cand else None
+    except ImportError:
+        return None
+
+
 def build_solvers(verbose=False):
     """make -C phist_b200/solvers (PHIST solver layers + drivers), if the
     PHIST sources are present; returns True when they were built"""
-    src = os.environ.get("PHIST_SRC", "/root/reference")
-    if not os.path.isdir(os.path.join(src, "src", "jada")):
+    src = os.environ.get("PHIST_SRC", "")
+    if not src or not os.path.isdir(os.path.join(src, "src", "jada")):
         return False
+    blas = openblas_path()
+    if not blas:
+        raise RuntimeError("no OpenBLAS shared library found (scipy's bundled libscipy_openblas); "
+                           "set OPENBLAS to its path")
     env = dict(os.environ, PHIST_SRC=src)
-    subprocess.run(["make", "-s", "-j8", "-C", os.path.join(HERE, "solvers"), "CXX_=g++", "CC_=gcc"],
-                   check=True, env=env)
+    subprocess.run(["make", "-s", "-j8", "-C", os.path.join(HERE, "solvers"), "CXX_=g++", "CC_=gcc",
+                    "OPENBLAS=" + blas], check=True, env=env)
     if verbose:
         print("built PHIST solver layers into", LIBDIR)
     return True

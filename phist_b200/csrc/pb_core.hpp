@@ -65,6 +65,9 @@ struct Error : std::runtime_error {
 };
 
 void report(const char* fcn, const char* msg);
+// looks up the allocation-free entry point's scratch address on the current
+// device (pb_noalloc.cu); called once at library initialisation
+void noalloc_setup_current_device();
 
 #define PB_THROW(code, ...)                                     \
   do {                                                          \

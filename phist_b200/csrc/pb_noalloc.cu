@@ -18,9 +18,13 @@
 //    scratch array exactly.  Larger m or k are rejected with -55.
 //  * The scratch array (4 MiB + 256 bytes) lives in every GPU that loads the
 //    library, for the life of the process.
-//  * The first call on a device looks up the array's device address with
-//    cudaGetSymbolAddress (a one-time set-up per device, done with that device
-//    current).  Make that first call before any stream capture begins.
+//  * The array's device address is looked up with cudaGetSymbolAddress once
+//    per device, with that device current.  phist_kernels_init does this for
+//    the device it selects; on any other device the first call does it, so
+//    make that first call before any stream capture begins.  The looked-up
+//    address is kept for the life of the process and is not looked up again
+//    after a cudaDeviceReset: a host application that resets a device must
+//    not call this entry point on that device afterwards.
 //  * All calls share the one array, which keeps the last call's contents.
 //    Calls that overlap on the GPU (for example on two streams at once) race
 //    on it and give wrong results; serialise them.
@@ -79,6 +83,15 @@ void fail(int* iflag, int code, const char* msg)
 }
 
 }  // namespace
+
+namespace pb {
+// eager per-device set-up for the device current at library initialisation
+void noalloc_setup_current_device()
+{
+  DeviceSlot* slot = nullptr;
+  if (device_slot(&slot) != cudaSuccess) cudaGetLastError();
+}
+}  // namespace pb
 
 extern "C" void phist_b200_DmvecT_times_mvec_noalloc(int64_t n, int m, int k, double alpha,
                                                      const double* V, int64_t ldv, const double* W,

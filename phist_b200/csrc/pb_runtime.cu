@@ -44,6 +44,7 @@ void Runtime::init()
   if (const char* v = getenv("PHIST_B200_GRAPHS")) use_graphs = atoi(v) != 0;
   if (const char* c = getenv("PHIST_B200_SELL_C")) sell_C = atoi(c);
   if (const char* s = getenv("PHIST_B200_SELL_SIGMA")) sell_sigma_default = atoll(s);
+  noalloc_setup_current_device();
   inited_ = true;
 }
 
