@@ -290,3 +290,29 @@ def test_single_precision_block_kernels(session, oracle):
     assert relerr(d, (V.astype(float) * W).sum(0)) < 1e-5
     for o in (Vh, Wh, C, mp):
         o.delete()
+
+
+@pytest.mark.parametrize("m,k", [(1, 1), (4, 4), (8, 8), (12, 12), (32, 32), (8, 5), (40, 24)])
+@pytest.mark.parametrize("n", [30011, 2097152])
+def test_fused_mvsdi_mvTmv_self(session, n, m, k):
+    """V and W the same block, as PHIST's orthogrrB passes them
+    (phist_orthogrr_def.hpp:291): W <- W C in place, then D = alpha W'W(:,:k) +
+    beta D with W read after the update -- the builtin's self variants
+    (gemm_kernels_fused_sCD.F90:516-543)"""
+    from phist_b200 import kernels as K
+    from phist_b200.objects import SdMat
+    rng = np.random.default_rng(m * 7 + k)
+    W = rng.uniform(-1, 1, (n, m))
+    Cm = rng.uniform(-1, 1, (m, k))
+    D0 = rng.uniform(-1, 1, (m, k))
+    mp, Wh = _mk(n, m, W)
+    C = SdMat(m, k).set(Cm)
+    D = SdMat(m, k).set(D0)
+    K.chk(K.phist_Dfused_mvsdi_mvTmv, 0.5, Wh.h, Wh.h, C.h, -1.0, D.h)
+    new = W.copy()
+    new[:, :k] = W @ Cm
+    out = Wh.get()
+    assert relerr(out, new) < TOL
+    assert relerr(D.get(), 0.5 * new.T @ new[:, :k] - D0) < TOL
+    for o in (Wh, C, D, mp):
+        o.delete()
