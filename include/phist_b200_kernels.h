@@ -425,6 +425,12 @@ void phist_b200_set_spmv_config(int nvec, int tpr, int unroll, int* iflag);
 /* block widths >= min_nvec (8..32) use the SpMMV kernel that stages the
  * gathered X rows in shared memory (values above 32 disable it) */
 void phist_b200_set_spmv_staged(int min_nvec, int* iflag);
+/* SpMMV on matrices whose rows have at most 8 entries: on = 1 (the default;
+ * environment PHIST_B200_SPMV_PREFETCH) runs a resident grid that copies the
+ * next tile's matrix entries into shared memory while the current tile
+ * gathers its X rows; on = 0 runs one tile per thread block.  Results are
+ * bitwise the same. */
+void phist_b200_set_spmv_prefetch(int on, int* iflag);
 /* batched CARP-CG: replay each iteration as a recorded CUDA graph (1, the
  * default; environment PHIST_B200_GRAPHS) or launch its kernels one by one
  * (0); both give bitwise identical results */

@@ -5,6 +5,7 @@
 #pragma once
 #include <cudaTypedefs.h>
 #include <algorithm>
+#include <atomic>
 #include <type_traits>
 #include <cmath>
 #include <numeric>
@@ -15,6 +16,7 @@
 #include "pb_core.hpp"
 #include "pb_spmmv.cuh"
 #include "pb_spmmv_staged.cuh"
+#include "pb_spmmv_pf.cuh"
 #include "pb_tile.cuh"
 #include "pb_dmma.cuh"
 
@@ -191,16 +193,22 @@ void mvec_upload(Mvec<T>* V)
   if (V->nrows == 0) return;
   T* h = V->h();
   // the host mirror is pageable: staged before the call returns (see sd_upload)
-  PB_CUDA(cudaMemcpy2DAsync(V->d(), V->lda * sizeof(T), h, V->lda * sizeof(T),
-                            V->nvec * sizeof(T), V->nrows, cudaMemcpyHostToDevice, stream()));
+  if (V->nvec == V->lda)
+    PB_CUDA(cudaMemcpyAsync(V->d(), h, sizeof(T) * (size_t)V->nrows * V->lda, cudaMemcpyHostToDevice, stream()));
+  else
+    PB_CUDA(cudaMemcpy2DAsync(V->d(), V->lda * sizeof(T), h, V->lda * sizeof(T),
+                              V->nvec * sizeof(T), V->nrows, cudaMemcpyHostToDevice, stream()));
 }
 template <class T>
 void mvec_download(Mvec<T>* V)
 {
   if (V->nrows == 0) return;
   T* h = V->h();
-  PB_CUDA(cudaMemcpy2DAsync(h, V->lda * sizeof(T), V->d(), V->lda * sizeof(T),
-                            V->nvec * sizeof(T), V->nrows, cudaMemcpyDeviceToHost, stream()));
+  if (V->nvec == V->lda)
+    PB_CUDA(cudaMemcpyAsync(h, V->d(), sizeof(T) * (size_t)V->nrows * V->lda, cudaMemcpyDeviceToHost, stream()));
+  else
+    PB_CUDA(cudaMemcpy2DAsync(h, V->lda * sizeof(T), V->d(), V->lda * sizeof(T),
+                              V->nvec * sizeof(T), V->nrows, cudaMemcpyDeviceToHost, stream()));
   rt().sync();
 }
 
@@ -212,8 +220,15 @@ void mvec_get_data(const void* vV, T* data, int32_t lda, int row_major)
   if (V->nrows == 0) return;
   if (row_major) {
     PB_REQUIRE(lda >= V->nvec, PB_INVALID_INPUT, "lda %d < nvec %d", lda, V->nvec);
-    PB_CUDA(cudaMemcpy2DAsync(data, (size_t)lda * sizeof(T), V->d(), V->lda * sizeof(T),
-                              V->nvec * sizeof(T), V->nrows, cudaMemcpyDeviceToHost, stream()));
+    if (lda == V->nvec && V->lda == V->nvec) {
+      // both sides contiguous: one linear copy (a 2D copy of n rows of a few
+      // bytes each runs far below the link rate)
+      PB_CUDA(cudaMemcpyAsync(data, V->d(), sizeof(T) * (size_t)V->nrows * V->nvec, cudaMemcpyDeviceToHost,
+                              stream()));
+    } else {
+      PB_CUDA(cudaMemcpy2DAsync(data, (size_t)lda * sizeof(T), V->d(), V->lda * sizeof(T),
+                                V->nvec * sizeof(T), V->nrows, cudaMemcpyDeviceToHost, stream()));
+    }
     rt().sync();
   } else {
     PB_REQUIRE(lda >= V->nrows, PB_INVALID_INPUT, "lda %d < nrows %d", lda, V->nrows);
@@ -236,8 +251,13 @@ void mvec_set_data(void* vV, const T* data, int32_t lda, int row_major)
   if (V->nrows == 0) return;
   if (row_major) {
     PB_REQUIRE(lda >= V->nvec, PB_INVALID_INPUT, "lda %d < nvec %d", lda, V->nvec);
-    PB_CUDA(cudaMemcpy2DAsync(V->d(), V->lda * sizeof(T), data, (size_t)lda * sizeof(T),
-                              V->nvec * sizeof(T), V->nrows, cudaMemcpyHostToDevice, stream()));
+    if (lda == V->nvec && V->lda == V->nvec) {
+      PB_CUDA(cudaMemcpyAsync(V->d(), data, sizeof(T) * (size_t)V->nrows * V->nvec, cudaMemcpyHostToDevice,
+                              stream()));
+    } else {
+      PB_CUDA(cudaMemcpy2DAsync(V->d(), V->lda * sizeof(T), data, (size_t)lda * sizeof(T),
+                                V->nvec * sizeof(T), V->nrows, cudaMemcpyHostToDevice, stream()));
+    }
     rt().sync();
   } else {
     PB_REQUIRE(lda >= V->nrows, PB_INVALID_INPUT, "lda %d < nrows %d", lda, V->nrows);
@@ -702,6 +722,23 @@ void launch_spmv_nv(const SparseMat<T>* A, const SellDev<T>& S, SpmvArgs<T>& p, 
       PB_LAUNCH_CHECK();
       return;
     }
+  }
+  if (fast && !dots && !p.u && rt().spmv_pf && (vec || (NV == 1 && p.nvec == 1))) {
+    // resident grid, next tile's entries prefetched into shared memory
+    constexpr int NT = TPR == 1 ? 128 : (TPR == 16 ? 512 : 256);
+    constexpr int RPBp = NT / TPR;
+    auto kern = k_sell_spmmv_pf<T, NV, TPR, NT>;
+    static std::atomic<int> occ{0};
+    if (occ.load() == 0) {
+      int o = 0;
+      PB_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&o, kern, NT, 0));
+      occ.store(std::max(1, o));
+    }
+    const int64_t ntiles = ceil_div(A->nchunks, RPBp / 32);
+    const int pgrid = (int)std::max<int64_t>(1, std::min<int64_t>(ntiles, (int64_t)rt().num_sms() * occ.load()));
+    kern<<<pgrid, NT, 0, stream()>>>(S, p);
+    PB_LAUNCH_CHECK();
+    return;
   }
 #define PB_SPMV(VECv, KMAXv, CCv)                                                         \
   if (dots)                                                                             \

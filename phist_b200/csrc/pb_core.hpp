@@ -191,6 +191,10 @@ class Runtime {
   // than the register kernel on the 3D Anderson matrix (nvec 8/16/32:
   // 219/436/1077 us against 152/285/545 us).
   int spmv_staged_min_nvec = 99;
+  // SpMMV on matrices with rows of at most 8 entries: resident grid with the
+  // next tile's entries prefetched into shared memory (pb_spmmv_pf.cuh);
+  // false: one tile per block (pb_spmmv.cuh)
+  bool spmv_pf = true;
   // stage block-vector tiles of the Gram kernels with TMA (else cp.async)
   bool use_tma = true;
   // FP64 block products on the tensor cores (DMMA) for widths multiple of 8

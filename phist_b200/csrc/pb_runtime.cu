@@ -44,6 +44,7 @@ void Runtime::init()
   if (const char* v = getenv("PHIST_B200_GRAPHS")) use_graphs = atoi(v) != 0;
   if (const char* c = getenv("PHIST_B200_SELL_C")) sell_C = atoi(c);
   if (const char* s = getenv("PHIST_B200_SELL_SIGMA")) sell_sigma_default = atoll(s);
+  if (const char* v = getenv("PHIST_B200_SPMV_PREFETCH")) spmv_pf = atoi(v) != 0;
   noalloc_setup_current_device();
   inited_ = true;
 }
@@ -525,6 +526,13 @@ void phist_b200_set_spmv_staged(int min_nvec, int* iflag)
 {
   PB_API_BEGIN(iflag);
   rt().spmv_staged_min_nvec = min_nvec;
+  PB_API_END(iflag);
+}
+
+void phist_b200_set_spmv_prefetch(int on, int* iflag)
+{
+  PB_API_BEGIN(iflag);
+  rt().spmv_pf = on != 0;
   PB_API_END(iflag);
 }
 

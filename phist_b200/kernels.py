@@ -119,6 +119,7 @@ _d("phist_b200_lane_count", [c_int_p, c_int_p])
 _d("phist_b200_device_memory", [_ct.POINTER(u64), _ct.POINTER(u64), c_int_p])
 _d("phist_b200_set_spmv_config", [c_int, c_int, c_int, c_int_p])
 _d("phist_b200_set_spmv_staged", [c_int, c_int_p])
+_d("phist_b200_set_spmv_prefetch", [c_int, c_int_p])
 _d("phist_b200_set_graphs", [c_int, c_int_p])
 _d("phist_b200_set_option", [_ct.c_char_p, c_int, c_int_p])
 _d("phist_b200_launch_count", [_ct.POINTER(u64), c_int_p])
