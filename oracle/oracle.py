@@ -283,6 +283,30 @@ def ref_ddot_prec(x, y):
     return res, resC
 
 
+def ref_gemm_sc_prec(V, W):
+    """PHIST's compensated V'W (dgemm_sc_prec_<m>_k, gemm_kernels_sC_prec.c)
+    for V with m in {1, 2, 4} columns, W with k columns; returns the
+    double-double result as its high and low parts (m x k each)"""
+    _, precl = ref_libs()
+    n, m = V.shape
+    k = W.shape[1]
+    assert m in (1, 2, 4)
+    bufs = []
+    for a in (V, W):
+        raw = np.zeros(a.size * 8 + 64, np.uint8)
+        off = (-raw.ctypes.data) % 64
+        b = raw[off:off + a.size * 8].view(np.float64).reshape(a.shape)
+        b[...] = a
+        bufs.append((raw, b))
+    res = np.zeros(m * k)
+    resC = np.zeros(m * k)
+    f = getattr(precl, "dgemm_sc_prec_%d_k" % m)
+    f.argtypes = [ct.c_int, ct.c_int] + [ct.c_void_p] * 4
+    f(n, k, _p(bufs[0][1]), _p(bufs[1][1]), _p(res), _p(resC))
+    # res[j*m + r] holds the (r, j) entry
+    return res.reshape(k, m).T.copy(), resC.reshape(k, m).T.copy()
+
+
 def jada_gmres(A, Q, R, sigma, tol, max_iter, max_bas, res_index=None):
     """GMRES for the Jacobi-Davidson correction equations, restated in numpy
     from PHIST's blocked GMRES as jadaCorrectionSolver_run drives it

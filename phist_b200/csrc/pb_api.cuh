@@ -17,6 +17,7 @@
 #include "pb_spmmv.cuh"
 #include "pb_spmmv_staged.cuh"
 #include "pb_spmmv_pf.cuh"
+#include "pb_prec.cuh"
 #include "pb_tile.cuh"
 #include "pb_dmma.cuh"
 
@@ -1031,6 +1032,45 @@ void mvtmv_async(MvTmvArgs<T>& a, int64_t n, int BM, int BK)
     case 32: mvtmv_async_bk<T, 32>(a, n, BK); break;
     default: mvtmv_async_bk<T, 64>(a, n, BK); break;
   }
+}
+
+// C = alpha*V'W + beta*C with compensated (double-double) sums, for
+// PHIST_ROBUST_REDUCTIONS (pb_prec.cuh); result blocks of at most 64 x 64
+inline void launch_mvTmv_prec(int64_t n, int m, int k, double alpha, const double* V, int64_t ldv,
+                              const double* W, int64_t ldw, double beta, double* Cd, int64_t ldc)
+{
+  for (int r0 = 0; r0 < m; r0 += 64)
+    for (int j0 = 0; j0 < k; j0 += 64) {
+      MvTmvPrecArgs a;
+      a.n = n;
+      a.m = std::min(64, m - r0);
+      a.k = std::min(64, k - j0);
+      a.V = V + r0; a.ldv = ldv;
+      a.W = W + j0; a.ldw = ldw;
+      a.alpha = alpha; a.beta = beta;
+      a.C = Cd + r0 + (int64_t)j0 * ldc; a.ldc = ldc;
+      const int nout = a.m * a.k;
+      const int nq = (int)ceil_div(nout, PREC_BS);
+      const int64_t ntiles = ceil_div(n, PREC_R);
+      const int grid = (int)std::max<int64_t>(1, std::min<int64_t>(ntiles, 2 * (int64_t)rt().num_sms()));
+      a.part = (double*)rt().scratch(sizeof(double) * 2 * (size_t)grid * nout);
+      a.counter = rt().counters();
+      if (nq <= 1) k_mvTmv_prec<1><<<grid, PREC_BS, 0, stream()>>>(a);
+      else if (nq <= 2) k_mvTmv_prec<2><<<grid, PREC_BS, 0, stream()>>>(a);
+      else if (nq <= 4) k_mvTmv_prec<4><<<grid, PREC_BS, 0, stream()>>>(a);
+      else if (nq <= 8) k_mvTmv_prec<8><<<grid, PREC_BS, 0, stream()>>>(a);
+      else k_mvTmv_prec<16><<<grid, PREC_BS, 0, stream()>>>(a);
+      PB_LAUNCH_CHECK();
+    }
+}
+
+// the Gram product a caller asked for: compensated sums when the caller sets
+// PHIST_ROBUST_REDUCTIONS in FP64 (PHIST's builtin has no FP32 robust
+// kernels either: its S/C/Z types are not implemented, builtin/kernels.cpp:270-283)
+template <class T>
+bool robust_requested(int flags_in)
+{
+  return (flags_in & PB_ROBUST_REDUCTIONS) && std::is_same<T, double>::value;
 }
 
 template <class T>

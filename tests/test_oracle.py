@@ -296,3 +296,25 @@ def test_oracle_carp_cgmn_solves_shifted_systems():
     for j in range(2):
         xs = np.linalg.solve(A - sig[j] * np.eye(n), b[:, j])
         assert np.linalg.norm(x[:, j] - xs) / np.linalg.norm(xs) < 1e-10
+
+
+@pytest.mark.parametrize("m,k", [(1, 3), (2, 5), (4, 4), (4, 9)])
+def test_mvTmv_prec_vs_phist(oracle, m, k):
+    """compensated Gram products: the oracle's Dot2 restatement against
+    PHIST's own dgemm_sc_prec_<m>_k (gemm_kernels_sC_prec.c) on
+    ill-conditioned columns (large cancelling terms), to a few ulp"""
+    _need_ref(oracle)
+    rng = np.random.default_rng(m * 10 + k)
+    n = 4096
+    V = rng.uniform(-1, 1, (n, m)) * np.exp(rng.uniform(-20, 20, (n, m)))
+    W = rng.uniform(-1, 1, (n, k))
+    hi, lo = oracle.ref_gemm_sc_prec(V, W)
+    C = oracle.mvTmv(V, W, prec=True)
+    ref = hi + lo
+    # Dot2 bound (Ogita-Rump-Oishi 2005, Prop. 5.3) for two differently
+    # ordered compensated sums: a few ulp of the result plus n eps^2 sum|v w|
+    bound = 8 * EPS * np.abs(ref) + 4 * n * EPS ** 2 * (np.abs(V).T @ np.abs(W))
+    assert np.all(np.abs(C - ref) <= bound)
+    # plain FP64 loses digits on these columns; the compensated sums do not
+    plain = oracle.mvTmv(V, W)
+    assert np.abs(plain - ref).max() > np.abs(C - ref).max()
