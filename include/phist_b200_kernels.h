@@ -172,6 +172,11 @@ void phist_##P##mvec_get_block(phist_##P##const_mvec_ptr V, phist_##P##mvec_ptr 
         int jmin, int jmax, int* iflag);                                         /* :378 */  \
 void phist_##P##mvec_set_block(phist_##P##mvec_ptr V, phist_##P##const_mvec_ptr Vblock,      \
         int jmin, int jmax, int* iflag);                                         /* :384 */  \
+/* V(:, off_i : off_i + n_i - 1) = W[i] for the blocks side by side, and back */              \
+void phist_##P##mvec_gather_mvecs(phist_##P##mvec_ptr V, phist_##P##const_mvec_ptr W[],         \
+        int nblocks, int* iflag);                                                /* :736 */   \
+void phist_##P##mvec_scatter_mvecs(phist_##P##const_mvec_ptr V, phist_##P##mvec_ptr W[],        \
+        int nblocks, int* iflag);                                                /* :737 */   \
 void phist_##P##sdMat_view_block(phist_##P##sdMat_ptr M, phist_##P##sdMat_ptr* Mblock,       \
         int imin, int imax, int jmin, int jmax, int* iflag);                     /* :402 */  \
 void phist_##P##sdMat_get_block(phist_##P##const_sdMat_ptr M, phist_##P##sdMat_ptr Mblock,   \

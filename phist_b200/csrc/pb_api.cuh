@@ -391,6 +391,7 @@ void sell_free(SparseMat<T>* A)
   rt().dfree(A->d_col);
   rt().dfree(A->d_val);
   rt().dfree(A->d_perm);
+  rt().dfree(A->d_iperm);
   rt().dfree(A->d_row_len);
   rt().dfree(A->d_diag);
 }
@@ -423,7 +424,9 @@ void sell_layout(SparseMat<T>* A, const std::vector<int64_t>& rp, const std::vec
   rt().dfree(A->d_col);
   rt().dfree(A->d_val);
   rt().dfree(A->d_perm);
+  rt().dfree(A->d_iperm);
   rt().dfree(A->d_row_len);
+  A->d_iperm = nullptr;
   A->d_chunk_ptr = nullptr;
   A->d_chunk_len = nullptr;
   A->d_col = nullptr;
@@ -487,6 +490,11 @@ void sell_layout(SparseMat<T>* A, const std::vector<int64_t>& rp, const std::vec
   A->d_col = (int32_t*)upload_vec(scol);
   A->d_val = (T*)upload_vec(sval);
   A->d_perm = ident ? nullptr : (int32_t*)upload_vec(perm);
+  if (!ident) {
+    std::vector<int32_t> iperm(nrows);
+    for (int64_t r = 0; r < nrows; r++) iperm[perm[r]] = (int32_t)r;
+    A->d_iperm = (int32_t*)upload_vec(iperm);
+  }
   A->d_row_len = (int32_t*)upload_vec(rlen);
   A->h_perm = std::move(perm);
   rt().sync();
@@ -802,6 +810,74 @@ void spmv_tile(const SparseMat<T>* A, SpmvArgs<T>& p, int nv)
       else launch_spmv_nv<T, 32, 8>(A, S, p, vec);
       break;
   }
+}
+
+// W = alpha*A*V + beta*W with W'W (Gw) and V'W (Gv) formed in the same pass
+// by the prefetching kernel (fused_spmv_mvTmv).  W may be NULL (beta = 0,
+// W not stored).  False when the single pass does not apply (width not a
+// power of two <= 32, unaligned or strided blocks, long rows, SELL C != 32):
+// the caller then runs SpMMV and the products as separate passes.
+template <class T, int NV, int TPR>
+void launch_spmv_gram_nv(const SparseMat<T>* A, SpmvArgs<T>& p, SdMat<T>* Gw, SdMat<T>* Gv)
+{
+  constexpr int NT = TPR == 1 ? 128 : 256;
+  constexpr int RPB = NT / TPR;
+  auto kern = k_sell_spmmv_pf<T, NV, TPR, NT, true>;
+  static std::atomic<int> occ{0};
+  if (occ.load() == 0) {
+    int o = 0;
+    PB_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&o, kern, NT, 0));
+    occ.store(std::max(1, o));
+  }
+  const int64_t ntiles = ceil_div(A->nchunks, RPB / 32);
+  const int grid = (int)std::max<int64_t>(1, std::min<int64_t>(ntiles, (int64_t)rt().num_sms() * occ.load()));
+  T* part = (T*)rt().scratch(sizeof(T) * 2 * (size_t)grid * NV * NV);
+  p.gram_w = Gw ? part : nullptr;
+  p.gram_v = Gv ? part + (size_t)grid * NV * NV : nullptr;
+  kern<<<grid, NT, 0, stream()>>>(sell_dev(A), p);
+  PB_LAUNCH_CHECK();
+  const int rb = (int)ceil_div(NV * NV, 32);
+  if (Gw) {
+    k_reduce_partials<T><<<rb, 256, 0, stream()>>>(p.gram_w, grid, NV * NV, Gw->d(), NV, Gw->lda, T(1), T(0));
+    PB_LAUNCH_CHECK();
+  }
+  if (Gv) {
+    k_reduce_partials<T><<<rb, 256, 0, stream()>>>(p.gram_v, grid, NV * NV, Gv->d(), NV, Gv->lda, T(1), T(0));
+    PB_LAUNCH_CHECK();
+  }
+}
+
+template <class T>
+bool spmv_gram_fused(T alpha, const SparseMat<T>* A, const Mvec<T>* V, T beta, Mvec<T>* W, SdMat<T>* Gw,
+                     SdMat<T>* Gv)
+{
+  const int nv = V->nvec;
+  const int NV = nv <= 1 ? 1 : nv <= 2 ? 2 : nv <= 4 ? 4 : nv <= 8 ? 8 : nv <= 16 ? 16 : nv <= 32 ? 32 : 0;
+  if (NV != nv || alpha == T(0) || A->nnz == 0 || !rt().spmv_pf) return false;
+  if (!(A->C == 32 && A->max_row_len <= 8)) return false;
+  const int vw = 16 / (int)sizeof(T);
+  if (NV >= 2 && (!aligned16<T>(V->d()) || V->lda % vw != 0)) return false;
+  if (NV >= 2 && W && (!aligned16<T>(W->d()) || W->lda % vw != 0)) return false;
+  if (sizeof(T) == 4 && NV == 2) return false;
+  SpmvArgs<T> p;
+  memset(&p, 0, sizeof(p));
+  p.alpha = alpha;
+  p.beta = W ? beta : T(0);
+  p.x = V->d();
+  p.ldx = V->lda;
+  p.y = W ? W->d() : nullptr;
+  p.ldy = W ? W->lda : 0;
+  p.nvec = nv;
+  p.no_store = W ? 0 : 1;
+  switch (NV) {
+    case 1: launch_spmv_gram_nv<T, 1, 1>(A, p, Gw, Gv); break;
+    case 2: launch_spmv_gram_nv<T, 2, 1>(A, p, Gw, Gv); break;
+    case 4: launch_spmv_gram_nv<T, 4, 1>(A, p, Gw, Gv); break;
+    case 8: launch_spmv_gram_nv<T, 8, 2>(A, p, Gw, Gv); break;
+    case 16: launch_spmv_gram_nv<T, 16, 4>(A, p, Gw, Gv); break;
+    default: launch_spmv_gram_nv<T, 32, 8>(A, p, Gw, Gv); break;
+  }
+  return true;
 }
 
 // general entry: tiles of <= 32 columns; dots returned to host arrays

@@ -300,6 +300,7 @@ struct SparseMat {
   int32_t* d_col = nullptr;
   T* d_val = nullptr;
   int32_t* d_perm = nullptr;       // SELL row -> original row
+  int32_t* d_iperm = nullptr;      // original row -> SELL row (nullptr: identity)
   int32_t* d_row_len = nullptr;    // per SELL row
   T* d_diag = nullptr;             // diagonal per original row (CARP)
   // host copy of the CRS structure (original order, for colouring/CARP)

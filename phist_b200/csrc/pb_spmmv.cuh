@@ -52,6 +52,12 @@ struct SpmvArgs {
   T gamma, delta;
   T* u;
   int64_t ldu;
+  // fused Gram products of the prefetching kernel (pb_spmmv_pf.cuh):
+  // per-block partial sums of W'W (gram_w) and V'W (gram_v), NV*NV each;
+  // store_y = 0 computes W only for the products (W = NULL in PHIST's call)
+  T* gram_w;
+  T* gram_v;
+  int no_store;
 };
 
 template <class T, int W>
@@ -358,6 +364,68 @@ k_sell_spmmv(SellDev<T> A, SpmvArgs<T> p)
     part[tid] = sacc;
   }
   last_block_reduce<T>(p.part, 2 * NV, gridDim.x, p.counter, p.dots_out, 1, 2 * NV, 0, T(1), T(0));
+}
+
+// Y = alpha*(s1_j A1 + s2_j A2) X + beta*Y in one pass (fused_spmv_pair,
+// phist_kernels_fused_decl.h:45-48).  Per element the arithmetic of PHIST's
+// composition (common/kernels_no_fused_spmv_pair.cpp): t1 = alpha*(A1 x)_ij,
+// y = s1_j*t1 + beta*y, t2 = alpha*(A2 x)_ij, y = s2_j*t2 + y, each product
+// summed in stored (column) order as in spmvm_kernels.F90:494-523.  Thread
+// per (row, column); the two matrices may have different SELL layouts, so
+// each row is found through the inverse row permutation.
+template <class T>
+struct PairArgs {
+  SellDev<T> A1, A2;
+  const int32_t* iperm1;
+  const int32_t* iperm2;
+  const int32_t* rlen1;
+  const int32_t* rlen2;
+  T alpha, beta;
+  T s1[32], s2[32];
+  const T* x;
+  int64_t ldx;
+  T* y;
+  int64_t ldy;
+  int64_t n;
+  int nvec;  // columns of this launch (<= 32), starting at x and y
+};
+
+template <class T>
+__device__ __forceinline__ typename Acc<T>::type sell_row_dot(const SellDev<T>& A, const int32_t* iperm,
+                                                              const int32_t* rlen, int64_t i, const T* x,
+                                                              int64_t ldx, int j)
+{
+  typedef typename Acc<T>::type AT;
+  const int64_t r = iperm ? (int64_t)iperm[i] : i;
+  const int64_t ch = r / A.C;
+  const int64_t base = A.chunk_ptr[ch] + (r - ch * A.C);
+  const int len = rlen[r];
+  AT acc = AT(0);
+  for (int k = 0; k < len; k++) {
+    const T a = __ldg(A.val + base + (int64_t)k * A.C);
+    const int64_t c = __ldg(A.col + base + (int64_t)k * A.C);
+    acc += AT(a) * AT(__ldg(x + c * ldx + j));
+  }
+  return acc;
+}
+
+template <class T>
+__global__ void __launch_bounds__(256) k_sell_spmmv_pair(PairArgs<T> p)
+{
+  typedef typename Acc<T>::type AT;
+  const int64_t tot = p.n * p.nvec;
+  for (int64_t t = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; t < tot; t += (int64_t)gridDim.x * blockDim.x) {
+    const int64_t i = t / p.nvec;
+    const int j = (int)(t - i * p.nvec);
+    const AT a1 = sell_row_dot(p.A1, p.iperm1, p.rlen1, i, p.x, p.ldx, j);
+    const AT a2 = sell_row_dot(p.A2, p.iperm2, p.rlen2, i, p.x, p.ldx, j);
+    const T t1 = T(AT(p.alpha) * a1);
+    const T t2 = T(AT(p.alpha) * a2);
+    T* yp = p.y + i * p.ldy + j;
+    T y = (p.beta == T(0)) ? p.s1[j] * t1 : p.s1[j] * t1 + p.beta * *yp;
+    y = p.s2[j] * t2 + y;
+    *yp = y;
+  }
 }
 
 // alpha == 0 / empty matrix: Y = beta*Y (crsmat_module.F90:1508-1511)

@@ -24,15 +24,36 @@
 // entries in stored order, y = alpha*tmp + beta*y (spmvm_kernels.F90:494-523);
 // results are bitwise those of the one-tile kernel.
 //
+// With GRAM set, the kernel also forms W'W and V'W of the new W in the same
+// pass (fused_spmv_mvTmv, phist_kernels_fused_decl.h:57-68): each tile's W
+// rows (and its own X rows, for V'W) are kept in shared memory, every thread
+// accumulates its share of the NV x NV products over the tile's rows, and
+// each block leaves its partial sums for a fixed-order second pass.
+//
 // Preconditions (checked by the launcher): SELL chunk height 32, at most 8
-// entries per row, no fused dot / axpby epilogue.
+// entries per row, no fused dot / axpby epilogue, the whole block vector as
+// the column tile when GRAM is set.
 #pragma once
 #include "pb_spmmv.cuh"
 #include "pb_tile.cuh"
 
 namespace pb {
 
-template <class T, int NV, int TPR, int NT>
+// a block's partial W'W and V'W: output o = c1 + NV*c2 (column-major NV x NV)
+template <class T, int NV, int NT, int NQ, class GT>
+__device__ __forceinline__ void gram_store(const SpmvArgs<T>& p, const GT* gw, const GT* gv)
+{
+#pragma unroll
+  for (int q = 0; q < NQ; q++) {
+    const int o = threadIdx.x + q * NT;
+    if (o < NV * NV) {
+      if (p.gram_w) p.gram_w[(int64_t)blockIdx.x * NV * NV + o] = T(gw[q]);
+      if (p.gram_v) p.gram_v[(int64_t)blockIdx.x * NV * NV + o] = T(gv[q]);
+    }
+  }
+}
+
+template <class T, int NV, int TPR, int NT, bool GRAM = false>
 __global__ void __launch_bounds__(NT) k_sell_spmmv_pf(SellDev<T> A, SpmvArgs<T> p)
 {
   constexpr int KMAX = 8, CC = 32;
@@ -48,6 +69,15 @@ __global__ void __launch_bounds__(NT) k_sell_spmmv_pf(SellDev<T> A, SpmvArgs<T> 
   __shared__ __align__(16) T sval[2][EPT];
   __shared__ __align__(16) int scol[2][EPT];
   __shared__ int64_t smeta[3][NCH + 1];  // chunk pointers of three tiles
+  // GRAM: the tile's new W rows and X rows (padded rows: no bank conflicts)
+  constexpr int GR = GRAM ? RPB : 1;
+  constexpr int NQ = GRAM ? (NV * NV + NT - 1) / NT : 1;  // products per thread
+  __shared__ T gys[GR][GRAM ? NV + 1 : 1];
+  __shared__ T gxs[GR][GRAM ? NV + 1 : 1];
+  typedef typename Acc<T>::type GT;
+  GT gw[NQ], gv[NQ];
+#pragma unroll
+  for (int q = 0; q < NQ; q++) { gw[q] = GT(0); gv[q] = GT(0); }
 
   const int tid = threadIdx.x;
   const int s = tid % TPR, lr = tid / TPR;
@@ -82,7 +112,10 @@ __global__ void __launch_bounds__(NT) k_sell_spmmv_pf(SellDev<T> A, SpmvArgs<T> 
   };
 
   int64_t t = blockIdx.x;
-  if (t >= ntiles) return;
+  if (t >= ntiles) {
+    if (GRAM) gram_store<T, NV, NT, NQ>(p, gw, gv);
+    return;
+  }
   {
     const int64_t m0 = meta_load(t);
     const int64_t m1 = meta_load(t + G);
@@ -104,15 +137,27 @@ __global__ void __launch_bounds__(NT) k_sell_spmmv_pf(SellDev<T> A, SpmvArgs<T> 
     cp_async_commit();
 
     const int64_t r = t * RPB + lr;  // SELL row
+    if (GRAM) {
+      // rows past the matrix add nothing to the products
+#pragma unroll
+      for (int v = 0; v < NVV; v++)
+#pragma unroll
+        for (int w = 0; w < VW; w++) {
+          gys[lr][spmv_col<TPR, VW>(s, v, w)] = T(0);
+          gxs[lr][spmv_col<TPR, VW>(s, v, w)] = T(0);
+        }
+    }
     if (r < nch * (int64_t)CC) {
       const int64_t i = (r < A.nrows) ? (A.perm ? (int64_t)A.perm[r] : r) : -1;
       AT acc[VPT];
 #pragma unroll
       for (int q = 0; q < VPT; q++) acc[q] = AT(0);
-      if (i >= 0 && p.has_shift) {
-        T xi[VPT];
+      T xi[VPT];
+      if (i >= 0 && (p.has_shift || (GRAM && p.gram_v))) {
 #pragma unroll
         for (int v = 0; v < NVV; v++) Vec<T, VW>::ld(x + i * p.ldx + spmv_col<TPR, VW>(s, v, 0), &xi[v * VW]);
+      }
+      if (i >= 0 && p.has_shift) {
 #pragma unroll
         for (int v = 0; v < NVV; v++)
 #pragma unroll
@@ -168,7 +213,31 @@ __global__ void __launch_bounds__(NT) k_sell_spmmv_pf(SellDev<T> A, SpmvArgs<T> 
 #pragma unroll
             for (int w = 0; w < VW; w++) yv[w] = T(AT(p.alpha) * acc[v * VW + w]);
           }
-          Vec<T, VW>::st(yr + c, yv);
+          if (!GRAM || !p.no_store) Vec<T, VW>::st(yr + c, yv);
+          if (GRAM) {
+#pragma unroll
+            for (int w = 0; w < VW; w++) {
+              gys[lr][c + w] = yv[w];
+              if (p.gram_v) gxs[lr][c + w] = xi[v * VW + w];
+            }
+          }
+        }
+      }
+    }
+    if (GRAM) {
+      // this tile's share of W'W and V'W, rows in tile order
+      __syncthreads();
+#pragma unroll
+      for (int q = 0; q < NQ; q++) {
+        const int o = tid + q * NT;
+        if (o < NV * NV) {
+          const int c1 = o % NV, c2 = o / NV;
+#pragma unroll 4
+          for (int rr = 0; rr < RPB; rr++) {
+            const T y2 = gys[rr][c2];
+            if (p.gram_w) gw[q] += GT(gys[rr][c1]) * GT(y2);
+            if (p.gram_v) gv[q] += GT(gxs[rr][c1]) * GT(y2);
+          }
         }
       }
     }
@@ -176,6 +245,7 @@ __global__ void __launch_bounds__(NT) k_sell_spmmv_pf(SellDev<T> A, SpmvArgs<T> 
     if (tid <= NCH) smeta[mbnn][tid] = mnext;
     __syncthreads();
   }
+  if (GRAM) gram_store<T, NV, NT, NQ>(p, gw, gv);
 }
 
 }  // namespace pb

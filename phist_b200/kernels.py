@@ -187,6 +187,8 @@ for _P, _ST in (("D", _ct.c_double), ("S", _ct.c_float)):
     _d(p + "mvec_view_block", [vp, vpp, c_int, c_int, c_int_p])
     _d(p + "mvec_get_block", [vp, vp, c_int, c_int, c_int_p])
     _d(p + "mvec_set_block", [vp, vp, c_int, c_int, c_int_p])
+    _d(p + "mvec_gather_mvecs", [vp, vpp, c_int, c_int_p])
+    _d(p + "mvec_scatter_mvecs", [vp, vpp, c_int, c_int_p])
     _d(p + "mvec_put_value", [vp, S, c_int_p])
     _d(p + "mvec_put_func", [vp, vp, vp, c_int_p])
     _d(p + "mvec_random", [vp, c_int_p])
