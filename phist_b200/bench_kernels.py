@@ -1,6 +1,6 @@
 """Per-kernel throughput of libphist_kernels_b200.so on the benchmark shapes.
 
-    python -m phist_b200.bench_kernels [--suite spmmv,block,blas,carp] [--reps R]
+    python -m phist_b200.bench_kernels [--suite spmmv,block,blas,carp] [--reps R] [--nvecs 1,...,32]
 
 Every kernel is called through the C ABI on device-resident data, timed with
 CUDA events on the library's stream, with the L2 flushed (256 MiB write)
@@ -70,12 +70,12 @@ def report(kernel, shape, nbytes, flops, t, peak):
 def suite_spmmv(T, reps, peak, L=128):
     from . import kernels as K
     from .generators import random_block
-    from .objects import Mvec, SparseMat
+    from .objects import Mvec, SdMat, SparseMat
     K.chk(K.phist_b200_set_sell_params, 32, 256)
     A = SparseMat.from_problem("ANDERSON3D-%d-S1" % L, flags=K.PHIST_SPARSEMAT_PERM_LOCAL)
     n, nnz = A.nrows, A.nnz
     out = []
-    for nv in (1, 2, 4, 8, 16, 32):
+    for nv in NVECS:
         X = Mvec(A.domain_map, nv).set(random_block(n, nv, 3))
         Y = Mvec(A.row_map, nv)
         sh = np.linspace(-1, 1, nv)
@@ -91,6 +91,14 @@ def suite_spmmv(T, reps, peak, L=128):
         t = T.time(lambda: K.chk(K.phist_Dfused_spmv_mvdot, 1.0, A.h, X.h, 0.0, Y.h,
                                  K.sptr(d1, np.float64), K.sptr(d2, np.float64)), reps)
         out.append(report("fused_spmv_mvdot", {"n": n, "nnz": nnz, "nvec": nv}, b, 2 * nnz * nv + 4 * n * nv, t, peak))
+        # W = A V with W'W and V'W in the same pass: the bytes of one SpMMV
+        Gw, Gv = SdMat(nv, nv), SdMat(nv, nv)
+        t = T.time(lambda: K.chk(K.phist_Dfused_spmv_mvTmv, 1.0, A.h, X.h, 0.0, Y.h, Gw.h, Gv.h,
+                                 flags=K.PHIST_SDMAT_RUN_ON_DEVICE), reps)
+        out.append(report("fused_spmv_mvTmv", {"n": n, "nnz": nnz, "nvec": nv}, b,
+                          2 * nnz * nv + 4 * n * nv * nv, t, peak))
+        Gw.delete()
+        Gv.delete()
         X.delete()
         Y.delete()
     A.delete()
@@ -165,6 +173,11 @@ def suite_block(T, reps, peak, n=1 << 21):
         t = T.time(lambda: K.chk(K.phist_Dfused_mvsd_mvTmv, 1.0, V.h, C.h, 0.0, W.h, G.h), reps)
         out.append(report("fused_mvsd_mvTmv", {"n": n, "m": m, "k": k}, 8 * n * (m + k),
                           2 * n * m * k + 2 * n * k * k, t, peak))
+        # compensated (double-double) Gram product, PHIST_ROBUST_REDUCTIONS
+        t = T.time(lambda: K.chk(K.phist_DmvecT_times_mvec, 1.0, V.h, W.h, 0.0, C.h,
+                                 flags=K.PHIST_ROBUST_REDUCTIONS | K.PHIST_SDMAT_RUN_ON_DEVICE), reps)
+        out.append(report("mvecT_times_mvec_robust", {"n": n, "m": m, "k": k}, 8 * n * (m + k),
+                          2 * n * m * k, t, peak))
         for o in (V, W, C, G):
             o.delete()
     m_.delete()
@@ -315,11 +328,17 @@ def suite_carp(T, reps, peak):
     return out
 
 
+NVECS = (1, 2, 4, 8, 16, 32)
+
+
 def main():
+    global NVECS
     ap = argparse.ArgumentParser()
     ap.add_argument("--suite", default="spmmv,block,blas,carp")
     ap.add_argument("--reps", type=int, default=10)
+    ap.add_argument("--nvecs", default="1,2,4,8,16,32", help="block widths of the spmmv suite")
     args = ap.parse_args()
+    NVECS = tuple(int(v) for v in args.nvecs.split(","))
     T = Timer()
     peak = _peak()
     for s in args.suite.split(","):

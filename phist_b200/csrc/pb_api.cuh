@@ -815,7 +815,7 @@ void spmv_tile(const SparseMat<T>* A, SpmvArgs<T>& p, int nv)
 // W = alpha*A*V + beta*W with W'W (Gw) and V'W (Gv) formed in the same pass
 // by the prefetching kernel (fused_spmv_mvTmv).  W may be NULL (beta = 0,
 // W not stored).  False when the single pass does not apply (width not a
-// power of two <= 32, unaligned or strided blocks, long rows, SELL C != 32):
+// power of two <= 16, unaligned or strided blocks, long rows, SELL C != 32):
 // the caller then runs SpMMV and the products as separate passes.
 template <class T, int NV, int TPR>
 void launch_spmv_gram_nv(const SparseMat<T>* A, SpmvArgs<T>& p, SdMat<T>* Gw, SdMat<T>* Gv)
@@ -852,7 +852,10 @@ bool spmv_gram_fused(T alpha, const SparseMat<T>* A, const Mvec<T>* V, T beta, M
                      SdMat<T>* Gv)
 {
   const int nv = V->nvec;
-  const int NV = nv <= 1 ? 1 : nv <= 2 ? 2 : nv <= 4 ? 4 : nv <= 8 ? 8 : nv <= 16 ? 16 : nv <= 32 ? 32 : 0;
+  // widths 1..16; at 32 the products (2*32*32 FMAs per row on the FP64
+  // tensor cores) make the single pass slower than SpMMV plus two Gram
+  // passes on the benchmark matrix (826 us against about 670 us)
+  const int NV = nv <= 1 ? 1 : nv <= 2 ? 2 : nv <= 4 ? 4 : nv <= 8 ? 8 : nv <= 16 ? 16 : 0;
   if (NV != nv || alpha == T(0) || A->nnz == 0 || !rt().spmv_pf) return false;
   if (!(A->C == 32 && A->max_row_len <= 8)) return false;
   const int vw = 16 / (int)sizeof(T);
@@ -874,8 +877,7 @@ bool spmv_gram_fused(T alpha, const SparseMat<T>* A, const Mvec<T>* V, T beta, M
     case 2: launch_spmv_gram_nv<T, 2, 1>(A, p, Gw, Gv); break;
     case 4: launch_spmv_gram_nv<T, 4, 1>(A, p, Gw, Gv); break;
     case 8: launch_spmv_gram_nv<T, 8, 2>(A, p, Gw, Gv); break;
-    case 16: launch_spmv_gram_nv<T, 16, 4>(A, p, Gw, Gv); break;
-    default: launch_spmv_gram_nv<T, 32, 8>(A, p, Gw, Gv); break;
+    default: launch_spmv_gram_nv<T, 16, 4>(A, p, Gw, Gv); break;
   }
   return true;
 }

@@ -36,22 +36,180 @@
 #pragma once
 #include "pb_spmmv.cuh"
 #include "pb_tile.cuh"
+#include "pb_dmma.cuh"
+#include <type_traits>
 
 namespace pb {
 
-// a block's partial W'W and V'W: output o = c1 + NV*c2 (column-major NV x NV)
-template <class T, int NV, int NT, int NQ, class GT>
-__device__ __forceinline__ void gram_store(const SpmvArgs<T>& p, const GT* gw, const GT* gv)
-{
+// Per-block accumulation of W'W and V'W over the tiles' rows kept in shared
+// memory (ys: new W rows, xs: the rows' own X rows, row pitch PY), and the
+// block's partial sums at the end: output o = c1 + NV*c2 (column-major
+// NV x NV) at gram_w / gram_v + blockIdx.x*NV*NV.
+//
+// Scalar form (any width): each thread holds a TM x TM micro-tile of both
+// products over one row group (rows g, g + RG, ... of every tile); NMT
+// micro-tiles x RG groups = NT threads; the groups are added in group order.
+template <class T, int NV, int NT, int RPB>
+struct GramScalar {
+  typedef typename Acc<T>::type GT;
+  static constexpr int PY = NV + 1;
+  static constexpr int TM = NV >= 4 ? 2 : 1;
+  static constexpr int NB = NV / TM;
+  static constexpr int NMT = NB * NB;
+  static constexpr int RG = NMT >= NT ? 1 : NT / NMT;
+  static_assert(NMT <= NT, "one micro-tile per thread at most");
+  static_assert(RPB * PY >= NT * TM * TM, "group partials fit the row buffer");
+  GT gw[TM][TM], gv[TM][TM];
+  int c1, c2, g;
+  __device__ __forceinline__ void init()
+  {
+    const int mt = (int)threadIdx.x % NMT;
+    g = (int)threadIdx.x / NMT;
+    c1 = (mt % NB) * TM;
+    c2 = (mt / NB) * TM;
 #pragma unroll
-  for (int q = 0; q < NQ; q++) {
-    const int o = threadIdx.x + q * NT;
-    if (o < NV * NV) {
-      if (p.gram_w) p.gram_w[(int64_t)blockIdx.x * NV * NV + o] = T(gw[q]);
-      if (p.gram_v) p.gram_v[(int64_t)blockIdx.x * NV * NV + o] = T(gv[q]);
+    for (int a = 0; a < TM; a++)
+#pragma unroll
+      for (int b = 0; b < TM; b++) { gw[a][b] = GT(0); gv[a][b] = GT(0); }
+  }
+  __device__ __forceinline__ void add_tile(const T* ys, const T* xs)
+  {
+    if (g >= RG) return;
+#pragma unroll 2
+    for (int rr = g; rr < RPB; rr += RG) {
+      T y1[TM], y2[TM], x1[TM];
+#pragma unroll
+      for (int a = 0; a < TM; a++) {
+        y1[a] = ys[rr * PY + c1 + a];
+        y2[a] = ys[rr * PY + c2 + a];
+        x1[a] = xs[rr * PY + c1 + a];
+      }
+#pragma unroll
+      for (int a = 0; a < TM; a++)
+#pragma unroll
+        for (int b = 0; b < TM; b++) {
+          gw[a][b] += GT(y1[a]) * GT(y2[b]);
+          gv[a][b] += GT(x1[a]) * GT(y2[b]);
+        }
     }
   }
-}
+  // buf: RPB*PY entries of shared memory, free on entry
+  __device__ __forceinline__ void store(const SpmvArgs<T>& p, T* buf)
+  {
+    for (int which = 0; which < 2; which++) {
+      T* out = which == 0 ? p.gram_w : p.gram_v;
+      __syncthreads();
+      if (out) {
+#pragma unroll
+        for (int a = 0; a < TM; a++)
+#pragma unroll
+          for (int b = 0; b < TM; b++)
+            buf[(threadIdx.x * TM + a) * TM + b] = T(which == 0 ? gw[a][b] : gv[a][b]);
+      }
+      __syncthreads();
+      if (out) {
+        for (int o = threadIdx.x; o < NV * NV; o += NT) {
+          const int i = o % NV, j = o / NV;
+          const int mt = (i / TM) + NB * (j / TM), a = i % TM, b = j % TM;
+          GT sum = GT(0);
+          for (int q = 0; q < RG; q++) sum += GT(buf[((q * NMT + mt) * TM + a) * TM + b]);
+          out[(int64_t)blockIdx.x * NV * NV + o] = T(sum);
+        }
+      }
+    }
+  }
+};
+
+// FP64 tensor-core form (NV a multiple of 16): the tile's Gram products as
+// DMMA m8n8k4 steps with the row index as the k dimension (fragment layout
+// as in pb_dmma.cuh: a = A[g][t], b = B[t][g], d = D[g][2t..2t+1]).  The
+// MT x MT output tiles of 8 x 8 are spread over the warps; where there are
+// fewer tiles than warps, warps with the same tile take interleaved 4-row
+// steps (KG groups) and are added in group order at the end.  Row pitch
+// NV + 4: the 4 rows of a fragment start 8 banks apart.
+template <int NV, int NT, int RPB>
+struct GramDmma {
+  static constexpr int PY = NV + 4;
+  static constexpr int MT = NV / 8;
+  static constexpr int NW = NT / 32;
+  static constexpr int TPW = MT * MT >= NW ? MT * MT / NW : 1;  // output tiles per warp
+  static constexpr int KG = MT * MT >= NW ? 1 : NW / (MT * MT);  // k-step groups
+  static constexpr int KS = RPB / 4;
+  static_assert(NV % 8 == 0 && RPB % 4 == 0 && KS % KG == 0, "bad DMMA Gram shape");
+  static_assert(RPB * PY >= KG * NV * NV, "group partials fit the row buffer");
+  double dw[TPW][2], dv[TPW][2];
+  int w, kg;
+  __device__ __forceinline__ void init()
+  {
+    w = (int)threadIdx.x >> 5;
+    kg = w / (MT * MT >= NW ? NW : MT * MT);
+#pragma unroll
+    for (int q = 0; q < TPW; q++) dw[q][0] = dw[q][1] = dv[q][0] = dv[q][1] = 0.0;
+  }
+  __device__ __forceinline__ int tile_of(int q) const
+  {
+    return MT * MT >= NW ? w * TPW + q : w % (MT * MT);
+  }
+  __device__ __forceinline__ void add_tile(const double* ys, const double* xs)
+  {
+    const int lane = threadIdx.x & 31, g8 = lane >> 2, t4 = lane & 3;
+#pragma unroll 2
+    for (int ks = kg; ks < KS; ks += KG) {
+      const int r = ks * 4 + t4;
+#pragma unroll
+      for (int q = 0; q < TPW; q++) {
+        const int tl = tile_of(q), i = tl % MT, j = tl / MT;
+        const double a = ys[r * PY + i * 8 + g8];
+        const double ax = xs[r * PY + i * 8 + g8];
+        const double b = ys[r * PY + j * 8 + g8];
+        dmma_884(dw[q][0], dw[q][1], a, b);
+        dmma_884(dv[q][0], dv[q][1], ax, b);
+      }
+    }
+  }
+  __device__ __forceinline__ void store(const SpmvArgs<double>& p, double* buf)
+  {
+    const int lane = threadIdx.x & 31, g8 = lane >> 2, t4 = lane & 3;
+    for (int which = 0; which < 2; which++) {
+      double* out = which == 0 ? p.gram_w : p.gram_v;
+      __syncthreads();
+      if (out) {
+#pragma unroll
+        for (int q = 0; q < TPW; q++) {
+          const int tl = tile_of(q), i = tl % MT, j = tl / MT;
+          const int c1 = i * 8 + g8, c2 = j * 8 + 2 * t4;
+          const double* d = which == 0 ? dw[q] : dv[q];
+          buf[kg * NV * NV + c1 + NV * c2] = d[0];
+          buf[kg * NV * NV + c1 + NV * (c2 + 1)] = d[1];
+        }
+      }
+      __syncthreads();
+      if (out) {
+        for (int o = threadIdx.x; o < NV * NV; o += NT) {
+          double sum = 0.0;
+          for (int q = 0; q < KG; q++) sum += buf[q * NV * NV + o];
+          out[(int64_t)blockIdx.x * NV * NV + o] = sum;
+        }
+      }
+    }
+  }
+};
+
+struct GramNone {
+  static constexpr int PY = 1;
+  __device__ __forceinline__ void init() {}
+};
+
+template <class T, int NV, int NT, int RPB>
+struct GramPick {
+  typedef GramScalar<T, NV, NT, RPB> type;
+};
+template <int NV, int NT, int RPB>
+struct GramPick<double, NV, NT, RPB> {
+  // widths 16 and 32 (at 8 the padded rows of the DMMA form exceed the
+  // static shared memory next to the prefetch buffers)
+  typedef typename std::conditional<NV % 16 == 0, GramDmma<NV, NT, RPB>, GramScalar<double, NV, NT, RPB>>::type type;
+};
 
 template <class T, int NV, int TPR, int NT, bool GRAM = false>
 __global__ void __launch_bounds__(NT) k_sell_spmmv_pf(SellDev<T> A, SpmvArgs<T> p)
@@ -69,15 +227,14 @@ __global__ void __launch_bounds__(NT) k_sell_spmmv_pf(SellDev<T> A, SpmvArgs<T> 
   __shared__ __align__(16) T sval[2][EPT];
   __shared__ __align__(16) int scol[2][EPT];
   __shared__ int64_t smeta[3][NCH + 1];  // chunk pointers of three tiles
-  // GRAM: the tile's new W rows and X rows (padded rows: no bank conflicts)
+  // GRAM: the tile's new W rows and X rows, and the block's accumulators
+  typedef typename std::conditional<GRAM, typename GramPick<T, NV, NT, RPB>::type, GramNone>::type Gram;
+  constexpr int PY = GRAM ? Gram::PY : 1;
   constexpr int GR = GRAM ? RPB : 1;
-  constexpr int NQ = GRAM ? (NV * NV + NT - 1) / NT : 1;  // products per thread
-  __shared__ T gys[GR][GRAM ? NV + 1 : 1];
-  __shared__ T gxs[GR][GRAM ? NV + 1 : 1];
-  typedef typename Acc<T>::type GT;
-  GT gw[NQ], gv[NQ];
-#pragma unroll
-  for (int q = 0; q < NQ; q++) { gw[q] = GT(0); gv[q] = GT(0); }
+  __shared__ __align__(16) T gys[GR * PY];
+  __shared__ __align__(16) T gxs[GR * PY];
+  Gram gram;
+  if constexpr (GRAM) gram.init();
 
   const int tid = threadIdx.x;
   const int s = tid % TPR, lr = tid / TPR;
@@ -113,7 +270,7 @@ __global__ void __launch_bounds__(NT) k_sell_spmmv_pf(SellDev<T> A, SpmvArgs<T> 
 
   int64_t t = blockIdx.x;
   if (t >= ntiles) {
-    if (GRAM) gram_store<T, NV, NT, NQ>(p, gw, gv);
+    if constexpr (GRAM) gram.store(p, gys);
     return;
   }
   {
@@ -137,14 +294,14 @@ __global__ void __launch_bounds__(NT) k_sell_spmmv_pf(SellDev<T> A, SpmvArgs<T> 
     cp_async_commit();
 
     const int64_t r = t * RPB + lr;  // SELL row
-    if (GRAM) {
+    if constexpr (GRAM) {
       // rows past the matrix add nothing to the products
 #pragma unroll
       for (int v = 0; v < NVV; v++)
 #pragma unroll
         for (int w = 0; w < VW; w++) {
-          gys[lr][spmv_col<TPR, VW>(s, v, w)] = T(0);
-          gxs[lr][spmv_col<TPR, VW>(s, v, w)] = T(0);
+          gys[lr * PY + spmv_col<TPR, VW>(s, v, w)] = T(0);
+          gxs[lr * PY + spmv_col<TPR, VW>(s, v, w)] = T(0);
         }
     }
     if (r < nch * (int64_t)CC) {
@@ -153,18 +310,34 @@ __global__ void __launch_bounds__(NT) k_sell_spmmv_pf(SellDev<T> A, SpmvArgs<T> 
 #pragma unroll
       for (int q = 0; q < VPT; q++) acc[q] = AT(0);
       T xi[VPT];
-      if (i >= 0 && (p.has_shift || (GRAM && p.gram_v))) {
+      if constexpr (GRAM) {
+        // the row's own X values: for the shift and for V'W
+        if (i >= 0 && (p.has_shift || p.gram_v)) {
 #pragma unroll
-        for (int v = 0; v < NVV; v++) Vec<T, VW>::ld(x + i * p.ldx + spmv_col<TPR, VW>(s, v, 0), &xi[v * VW]);
-      }
-      if (i >= 0 && p.has_shift) {
+          for (int v = 0; v < NVV; v++) Vec<T, VW>::ld(x + i * p.ldx + spmv_col<TPR, VW>(s, v, 0), &xi[v * VW]);
+        }
+        if (i >= 0 && p.has_shift) {
 #pragma unroll
-        for (int v = 0; v < NVV; v++)
+          for (int v = 0; v < NVV; v++)
 #pragma unroll
-          for (int w = 0; w < VW; w++) {
-            const int c = spmv_col<TPR, VW>(s, v, w);
-            acc[v * VW + w] = AT(p.sh[c]) * AT(xi[v * VW + w]);
-          }
+            for (int w = 0; w < VW; w++) {
+              const int c = spmv_col<TPR, VW>(s, v, w);
+              acc[v * VW + w] = AT(p.sh[c]) * AT(xi[v * VW + w]);
+            }
+        }
+      } else {
+        if (i >= 0 && p.has_shift) {
+          T xs[VPT];
+#pragma unroll
+          for (int v = 0; v < NVV; v++) Vec<T, VW>::ld(x + i * p.ldx + spmv_col<TPR, VW>(s, v, 0), &xs[v * VW]);
+#pragma unroll
+          for (int v = 0; v < NVV; v++)
+#pragma unroll
+            for (int w = 0; w < VW; w++) {
+              const int c = spmv_col<TPR, VW>(s, v, w);
+              acc[v * VW + w] = AT(p.sh[c]) * AT(xs[v * VW + w]);
+            }
+        }
       }
       const int lc = lr / CC, l = lr % CC;
       const int cb = (int)(smeta[mb][lc] - smeta[mb][0]) + l;
@@ -214,38 +387,26 @@ __global__ void __launch_bounds__(NT) k_sell_spmmv_pf(SellDev<T> A, SpmvArgs<T> 
             for (int w = 0; w < VW; w++) yv[w] = T(AT(p.alpha) * acc[v * VW + w]);
           }
           if (!GRAM || !p.no_store) Vec<T, VW>::st(yr + c, yv);
-          if (GRAM) {
+          if constexpr (GRAM) {
 #pragma unroll
             for (int w = 0; w < VW; w++) {
-              gys[lr][c + w] = yv[w];
-              if (p.gram_v) gxs[lr][c + w] = xi[v * VW + w];
+              gys[lr * PY + c + w] = yv[w];
+              if (p.gram_v) gxs[lr * PY + c + w] = xi[v * VW + w];
             }
           }
         }
       }
     }
-    if (GRAM) {
-      // this tile's share of W'W and V'W, rows in tile order
+    if constexpr (GRAM) {
+      // this tile's share of W'W and V'W
       __syncthreads();
-#pragma unroll
-      for (int q = 0; q < NQ; q++) {
-        const int o = tid + q * NT;
-        if (o < NV * NV) {
-          const int c1 = o % NV, c2 = o / NV;
-#pragma unroll 4
-          for (int rr = 0; rr < RPB; rr++) {
-            const T y2 = gys[rr][c2];
-            if (p.gram_w) gw[q] += GT(gys[rr][c1]) * GT(y2);
-            if (p.gram_v) gv[q] += GT(gxs[rr][c1]) * GT(y2);
-          }
-        }
-      }
+      gram.add_tile(gys, gxs);
     }
     cp_async_wait<0>();
     if (tid <= NCH) smeta[mbnn][tid] = mnext;
     __syncthreads();
   }
-  if (GRAM) gram_store<T, NV, NT, NQ>(p, gw, gv);
+  if constexpr (GRAM) gram.store(p, gys);
 }
 
 }  // namespace pb
