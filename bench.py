@@ -197,6 +197,60 @@ def jada_forms(timeout=300):
     return {"workload": "subspacejada_laplace3d_64_10eigs", "n": 262144, "tol": 1e-10, "forms": forms}
 
 
+def served_forms(timeout=300):
+    """A short served request stream (the served-stream configuration with
+    fewer and smaller requests so that it fits the benchmark's time):
+    Poisson arrivals at 200/s (stream seed 5) of eigen-solves, each the 8
+    smallest eigenpairs (tol 1e-10) of a 7-point Laplacian + diag uniform[0,1)
+    on an L^3 grid, L log-uniform in [24, 64], through
+    phist_b200/lib/serve_run (PHIST's unchanged subspacejada per request).
+    Forms: plain FP64 drop-in on one stream; FP64 and FP32-correction
+    solves on the device GMRES served by 8 workers on their own lanes."""
+    exe = os.path.join(ROOT, "phist_b200", "lib", "serve_run")
+    if not os.path.exists(exe):
+        return {"unavailable": "phist_b200/lib/serve_run is not built (phist_b200/solvers/Makefile)"}
+    common = ["nreq=12", "rate=200", "lmin=24", "lmax=64", "seed=5", "numEigs=8", "tol=1e-10"]
+    forms = {}
+    for name, extra in (("fp64_one_stream", ["workers=1", "devgmres=0"]),
+                        ("fp64_device_gmres_served", ["workers=8", "devgmres=1"]),
+                        ("mixed_device_gmres_served", ["workers=8", "devgmres=1", "mixed=1"])):
+        try:
+            r = subprocess.run([exe] + common + extra, capture_output=True, text=True, timeout=timeout)
+            d = json.loads([ln for ln in r.stdout.splitlines() if ln.startswith("{")][-1])
+        except Exception as e:  # a failed form is reported, not fatal to the bench line
+            forms[name] = {"failed": str(e)[:200]}
+            continue
+        forms[name] = {k: d.get(k) for k in ("solves_per_s", "latency_p50", "latency_p99", "latency_mean", "wall",
+                                             "failed", "unconverged", "max_resExplicit") if k in d}
+    return {"workload": "served_laplace_diag_stream_12req_L24_64", "requests": 12, "forms": forms}
+
+
+def carp_forms(reps=5):
+    """Batched multi-shift CARP-CG on the 1024 x 1024 x 2 honeycomb lattice
+    (n = 2,097,152, on-site uniform[-0.5,0.5) seed 4): device time of one
+    iteration (forward+backward colour sweep and fused CG updates) per slot
+    count 1..32, FP64 and with FP32 sweeps, from the library's slot tuner
+    (phist_b200_DcarpCG_tune_block), and the slot count it picks for 32
+    systems.  Solves to 1e-10 of these indefinite systems need far more
+    iterations than a benchmark run allows, so the figure is per iteration."""
+    import ctypes as ct
+
+    from phist_b200 import kernels as K
+    from phist_b200.objects import SparseMat
+    A = SparseMat.from_problem("HONEYCOMB-1024-S4-W1")
+    out = {"workload": "carpcg_honeycomb_1024x1024x2_32_shifts", "n": A.nrows, "nnz": A.nnz}
+    for name, mixed in (("fp64", 0), ("fp32_sweeps", 1)):
+        us = (ct.c_double * 6)()
+        blk = ct.c_int(0)
+        K.chk(K.phist_b200_DcarpCG_tune_block, A.h, 32, mixed, reps, ct.byref(blk), us)
+        t = {str(1 << q): round(us[q], 1) for q in range(6) if us[q] > 0}
+        best = blk.value
+        out[name] = {"iteration_us": t, "block": best,
+                     "system_iterations_per_s": round(best / (us[best.bit_length() - 1] * 1e-6), 1)}
+    A.delete()
+    return out
+
+
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
@@ -207,6 +261,7 @@ def main():
     ap.add_argument("--nvecs", default=",".join(map(str, NVECS)))
     ap.add_argument("--no-jada", action="store_true", help="skip the eigen-solve timings")
     ap.add_argument("--no-e2e", action="store_true", help="skip the end-to-end runs through host buffers")
+    ap.add_argument("--no-forms", action="store_true", help="skip the served-stream and CARP-CG timings")
     args = ap.parse_args()
     nvecs = [int(t) for t in args.nvecs.split(",")]
 
@@ -403,6 +458,12 @@ def main():
                                 if k != "seconds"}
     if rank == 0 and world == 1 and not args.no_jada:
         line["jada"] = jada_forms()
+    if rank == 0 and world == 1 and not args.no_forms:
+        line["served"] = served_forms()
+        try:
+            line["carp_cg"] = carp_forms()
+        except Exception as e:  # reported, not fatal to the bench line
+            line["carp_cg"] = {"failed": str(e)[:200]}
     if rank == 0:
         print(json.dumps(line), flush=True)
     for k in nvecs:
