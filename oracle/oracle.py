@@ -34,6 +34,36 @@ def build(with_ref=None):
     subprocess.run(["make", "-s", "-C", HERE] + targets, check=True, env=env)
 
 
+JADA_CPU = os.path.join(HERE, "_ref", "jada_run_cpu")
+
+
+def build_cpu():
+    """make -C oracle cpu: PHIST's FP64 solver layers on the CPU backend
+    (cpu_backend.cpp) and the jada_run driver, when the PHIST sources
+    (PHIST_SRC) and the solver objects are present"""
+    src = os.environ.get("PHIST_SRC", "")
+    if not src or not os.path.isdir(os.path.join(src, "src", "jada")):
+        return False
+    from phist_b200.build import openblas_path
+    env = dict(os.environ, PHIST_SRC=src, OPENBLAS=openblas_path() or "")
+    subprocess.run(["make", "-s", "-C", HERE, "cpu"], check=True, env=env)
+    return True
+
+
+def jada_cpu(args, threads=None, timeout=600):
+    """runs PHIST's subspacejada on the CPU backend (oracle/_ref/jada_run_cpu)
+    with the driver arguments of phist_b200/lib/jada_run; returns its JSON"""
+    import json
+    env = dict(os.environ)
+    if threads:
+        env["OMP_NUM_THREADS"] = str(threads)
+    r = subprocess.run([JADA_CPU] + list(args), capture_output=True, text=True, timeout=timeout, env=env)
+    lines = [ln for ln in r.stdout.splitlines() if ln.startswith("{")]
+    if r.returncode != 0 or not lines:
+        raise RuntimeError("jada_run_cpu failed (%d): %s" % (r.returncode, r.stderr[-500:]))
+    return json.loads(lines[-1])
+
+
 _lib = None
 
 
