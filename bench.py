@@ -197,18 +197,18 @@ def jada_forms(timeout=300):
     out = {"workload": "subspacejada_laplace3d_64_10eigs", "n": 262144, "tol": 1e-10, "forms": forms}
     # the same solve (PHIST's unchanged subspacejada, same options and start
     # block) on the host cores: the CPU restatement of PHIST's builtin kernels
-    # (oracle/cpu_backend.cpp); one warm solve is the sample
+    # (oracle/cpu_backend.cpp); one solve is the sample
     try:
         from oracle import oracle as O
         if os.path.exists(O.JADA_CPU):
             cores = os.cpu_count() or 1
-            d = O.jada_cpu(common[:-1] + ["reps=2"], threads=cores, timeout=timeout)
+            d = O.jada_cpu(common[:-1] + ["reps=1"], threads=cores, timeout=timeout)
             sec = d["wall"][-1]
             out["cpu_baseline"] = {
                 "seconds": round(sec, 4), "solves_per_s": round(1.0 / sec, 4), "cores": cores, "kind": "port",
                 "outer_iterations": d["nIter"], "converged": d["nConv"],
                 "max_res_explicit": max(d["resExplicit"][:10]),
-                "sample": "one warm FP64 solve of the same problem: PHIST's subspacejada (unchanged, from its "
+                "sample": "one FP64 solve of the same problem: PHIST's subspacejada (unchanged, from its "
                           "sources) on a host-core restatement of PHIST's builtin kernels, OpenMP"}
             for name, f in forms.items():
                 if "seconds" in f:
