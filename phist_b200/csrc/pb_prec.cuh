@@ -11,7 +11,8 @@
 // Comput. 26(6), 2005): every product is split exactly into p + e by an FMA
 // (TwoProduct), p is added to the running sum with TwoSum, and the rounding
 // errors of both are collected in a second accumulator.  Blocks stage row
-// tiles of V and W in shared memory; each thread owns up to NQ outputs.
+// tiles of V and W in shared memory; each thread owns up to NQ outputs, or,
+// for fewer outputs than threads, one output and a group of the tile's rows.
 // Per-block (sum, error) pairs are combined by the last block to arrive, in
 // block order with TwoSum, so the result does not depend on the schedule.
 // Finally C = alpha*(s + c) + beta*C is evaluated in double-double and
@@ -65,6 +66,10 @@ struct MvTmvPrecArgs {
 constexpr int PREC_BS = 256;
 constexpr int PREC_R = 32;  // rows per staged tile
 
+// Thread t owns output o = t mod nout (NQ = 1, nout <= PREC_BS) and takes the
+// rows g, g + G, ... of every tile, g = t / nout, G = PREC_BS / nout row
+// groups; with more outputs than threads (NQ > 1) every thread owns NQ
+// outputs and all rows.  The groups are combined in group order at the end.
 template <int NQ>
 __global__ void __launch_bounds__(PREC_BS) k_mvTmv_prec(MvTmvPrecArgs a)
 {
@@ -72,13 +77,16 @@ __global__ void __launch_bounds__(PREC_BS) k_mvTmv_prec(MvTmvPrecArgs a)
   __shared__ double ws[PREC_R][64 + 1];
   const int tid = threadIdx.x;
   const int m = a.m, k = a.k, nout = m * k;
+  const int G = NQ == 1 ? PREC_BS / nout : 1;  // row groups
+  const int g = NQ == 1 ? tid / nout : 0;
+  const bool active = g < G;
   double s[NQ], c[NQ];
   int orow[NQ], ocol[NQ];
 #pragma unroll
   for (int q = 0; q < NQ; q++) {
     s[q] = 0.0;
     c[q] = 0.0;
-    const int o = tid + q * PREC_BS;
+    const int o = NQ == 1 ? tid % nout : tid + q * PREC_BS;
     orow[q] = o < nout ? o % m : 0;
     ocol[q] = o < nout ? o / m : 0;
   }
@@ -96,17 +104,33 @@ __global__ void __launch_bounds__(PREC_BS) k_mvTmv_prec(MvTmvPrecArgs a)
       ws[ii][j] = ii < rows ? a.W[(i0 + ii) * a.ldw + j] : 0.0;
     }
     __syncthreads();
-    for (int ii = 0; ii < rows; ii++) {
+    if (active) {
+      for (int ii = g; ii < rows; ii += G) {
 #pragma unroll
-      for (int q = 0; q < NQ; q++)
-        if (tid + q * PREC_BS < nout) dd_dot_step(vs[ii][orow[q]], ws[ii][ocol[q]], s[q], c[q]);
+        for (int q = 0; q < NQ; q++)
+          if (NQ == 1 || tid + q * PREC_BS < nout) dd_dot_step(vs[ii][orow[q]], ws[ii][ocol[q]], s[q], c[q]);
+      }
+    }
+  }
+  if (NQ == 1 && G > 1) {
+    // row groups of one output, combined in group order
+    double* red = &vs[0][0];  // 2*PREC_BS <= PREC_R*65 entries
+    __syncthreads();
+    red[2 * tid] = s[0];
+    red[2 * tid + 1] = c[0];
+    __syncthreads();
+    if (tid < nout) {
+      double ss = 0.0, cc = 0.0;
+      for (int q = 0; q < G; q++) dd_add(ss, cc, red[2 * (q * nout + tid)], red[2 * (q * nout + tid) + 1]);
+      s[0] = ss;
+      c[0] = cc;
     }
   }
   double* part = a.part + (int64_t)blockIdx.x * nout * 2;
 #pragma unroll
   for (int q = 0; q < NQ; q++) {
     const int o = tid + q * PREC_BS;
-    if (o < nout) {
+    if (o < nout && (NQ > 1 || g == 0)) {
       part[2 * o] = s[q];
       part[2 * o + 1] = c[q];
     }
