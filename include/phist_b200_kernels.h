@@ -320,9 +320,11 @@ void phist_b200_##P##sparseMat_sell_info(phist_##P##const_sparseMat_ptr A, int* 
 /* raw device pointers of an mvec / sdMat view (element (0,0)) and its lda       */         \
 void phist_b200_##P##mvec_device_view(phist_##P##mvec_ptr V, ST** d_ptr, phist_lidx* lda,    \
         int* iflag);                                                                         \
-/* rows of the colour-ordered CARP sweep set up by carp_setup: colour classes   */          \
-/* in increasing colour, rows ascending inside a class; color_ptr has ncolors+1 */          \
-/* entries (pass NULL for outputs that are not wanted)                           */          \
+/* row order of the CARP sweep set up by carp_setup: the forward sweep equals   */          \
+/* the sequential Kaczmarz sweep over `rows`, the backward sweep the one over   */          \
+/* its reverse; rows[color_ptr[k] .. color_ptr[k+1]) is a distance-2            */          \
+/* independent set (ncolors sets, color_ptr has ncolors+1 entries; pass NULL    */          \
+/* for outputs that are not wanted)                                              */          \
 void phist_b200_##P##carp_color_order(void* const work, int32_t* rows, int* ncolors,         \
         int64_t* color_ptr, int* iflag);
 
@@ -443,8 +445,12 @@ void phist_b200_set_graphs(int on, int* iflag);
 /* kernel-path switches, all on by default (1) and each also read from the
  * environment at init: "tma" (TMA-staged block products, PHIST_B200_TMA),
  * "dmma" (FP64 tensor-core tiles, PHIST_B200_DMMA), "graphs" (as
- * phist_b200_set_graphs, PHIST_B200_GRAPHS).  "graphs" never changes a
- * result; tma/dmma change the summation order of the block products.
+ * phist_b200_set_graphs, PHIST_B200_GRAPHS), "carp_blocks" (CARP sweeps
+ * over a block colouring with X staged in shared memory, else one launch per
+ * row colour class; PHIST_B200_CARP_BLOCKS; applies to CARP work set up
+ * afterwards).  "graphs" never changes a result; tma/dmma change the
+ * summation order of the block products; carp_blocks changes the row order
+ * of the sweep (phist_b200_Dcarp_color_order reports it).
  * Unknown names: PHIST_INVALID_INPUT. */
 void phist_b200_set_option(const char* name, int value, int* iflag);
 /* SpMMV autotuner (no PHIST counterpart: GHOST fixes C = 32 on CUDA and sigma

@@ -303,27 +303,34 @@ def _autotune_one(T, reps, peak, prob):
 
 
 def suite_carp(T, reps, peak):
+    """double CARP sweep on the honeycomb matrix (1024 x 1024 cells, 2 sites),
+    block-coloured layout (default) and row-colour layout, 8 and 16 shifts"""
     from . import kernels as K
     from .generators import random_block
     from .objects import Mvec, SparseMat
     A = SparseMat.from_problem("HONEYCOMB-1024-S4-W1")
     n, nnz = A.nrows, A.nnz
-    nv = 8
-    sh = np.linspace(-2.5, 2.5, nv)
-    om = np.ones(nv)
-    work = ct.c_void_p()
-    K.chk(K.phist_Dcarp_setup, A.h, nv, K.sptr(sh, np.float64), ct.byref(work))
-    X = Mvec(A.row_map, nv)
-    B = Mvec(A.row_map, nv).set(random_block(n, nv, 4))
-    t = T.time(lambda: K.chk(K.phist_Dcarp_sweep, A.h, K.sptr(sh, np.float64), B.h, X.h, work,
-                             K.sptr(om, np.float64)), reps)
-    nb = 2 * (nnz * 12 + 8 * n * nv * 3)
-    nc = ct.c_int()
-    K.chk(K.phist_b200_Dcarp_color_order, work, None, ct.byref(nc), None)
-    out = [report("carp_sweep", {"n": n, "nnz": nnz, "nvec": nv, "colors": nc.value}, nb, 16 * nnz * nv, t, peak)]
-    K.chk(K.phist_Dcarp_destroy, A.h, work)
-    X.delete()
-    B.delete()
+    out = []
+    for blocks in (1, 0):
+        K.chk(K.phist_b200_set_option, b"carp_blocks", blocks)
+        for nv in (8, 16):
+            sh = np.linspace(-2.5, 2.5, nv)
+            om = np.ones(nv)
+            work = ct.c_void_p()
+            K.chk(K.phist_Dcarp_setup, A.h, nv, K.sptr(sh, np.float64), ct.byref(work))
+            X = Mvec(A.row_map, nv)
+            B = Mvec(A.row_map, nv).set(random_block(n, nv, 4))
+            t = T.time(lambda: K.chk(K.phist_Dcarp_sweep, A.h, K.sptr(sh, np.float64), B.h, X.h, work,
+                                     K.sptr(om, np.float64)), reps)
+            nb = 2 * (nnz * 12 + 8 * n * nv * 3)
+            nc = ct.c_int()
+            K.chk(K.phist_b200_Dcarp_color_order, work, None, ct.byref(nc), None)
+            out.append(report("carp_sweep", {"n": n, "nnz": nnz, "nvec": nv, "layout": "blocks" if blocks else "rowcolour",
+                                             "segments": nc.value}, nb, 16 * nnz * nv, t, peak))
+            K.chk(K.phist_Dcarp_destroy, A.h, work)
+            X.delete()
+            B.delete()
+    K.chk(K.phist_b200_set_option, b"carp_blocks", 1)
     A.delete()
     return out
 

@@ -1472,6 +1472,39 @@ RowGemmArgs<T> rowgemm_args()
 // ======================================================================
 // CARP
 // ======================================================================
+// Block-coloured layout (pb_carp_blocks.hpp): blocks of at most 128 rows
+// whose footprint has at most 256 rows of X and whose pattern at most 2048
+// entries.  False when the matrix has rows too long for that, or a block
+// needs more than 64 steps; the caller then uses the row colouring.
+template <class T>
+bool carp_build_blocks(const SparseMat<T>* A, const std::vector<int64_t>& prp, const std::vector<int32_t>& pcol,
+                       CarpWork<T>* w)
+{
+  const int64_t n = A->nrows;
+  CarpBlocks B;
+  if (!carp_block_partition(n, prp, pcol, 128, 256, 2048, B)) return false;
+  if (!carp_block_color(n, prp, pcol, B)) return false;
+  CarpBlockLayout<T> L;
+  carp_block_layout<T>(B, n, A->h_row_ptr.data(), A->h_col.data(), A->h_val.data(), L);
+  w->blocks = true;
+  w->nbcolors = B.ncolors;
+  w->h_bcolor_ptr = B.color_ptr;
+  w->max_fp = B.max_fp;
+  w->max_rows = B.max_rows;
+  w->max_nnz = L.max_nnz;
+  w->h_rows = B.seq_rows;
+  w->h_color_ptr = B.seq_ptr;
+  w->ncolors = (int)B.seq_ptr.size() - 1;
+  w->d_desc = (CarpBlockDesc*)upload_vec(L.desc);
+  w->d_bfp = (int32_t*)upload_vec(L.fp);
+  w->d_bval = (T*)upload_vec(L.val);
+  w->d_blcol = (uint16_t*)upload_vec(L.lcol);
+  w->d_blrp = (uint16_t*)upload_vec(L.lrp);
+  w->d_bnd = (T*)upload_vec(L.nd);
+  w->d_bstep = (uint16_t*)upload_vec(L.step);
+  return true;
+}
+
 template <class T>
 CarpWork<T>* carp_build(const SparseMat<T>* A, int nshifts, const T* sr, const T* si)
 {
@@ -1496,6 +1529,11 @@ CarpWork<T>* carp_build(const SparseMat<T>* A, int nshifts, const T* sr, const T
     }
     if (!has_diag) pcol.push_back((int32_t)i);
     prp[i + 1] = (int64_t)pcol.size();
+  }
+  w->nrows = n;
+  if (rt().carp_blocks && n > 0 && carp_build_blocks(A, prp, pcol, w)) {
+    rt().sync();
+    return w;
   }
   std::vector<int32_t> color;
   w->ncolors = dist2_color(n, A->ncols, prp, pcol, color);
@@ -1525,7 +1563,7 @@ CarpWork<T>* carp_build(const SparseMat<T>* A, int nshifts, const T* sr, const T
     dg[q] = d;
     rp[q + 1] = (int64_t)col.size();
   }
-  w->nrows = n;
+  w->h_rows = rows;
   w->d_rows = (int32_t*)upload_vec(rows);
   w->d_rp = (int64_t*)upload_vec(rp);
   w->d_col = (int32_t*)upload_vec(col);
@@ -1546,13 +1584,80 @@ void carp_free(CarpWork<T>* w)
   rt().dfree(w->d_val);
   rt().dfree(w->d_nrm);
   rt().dfree(w->d_diag);
+  rt().dfree(w->d_desc);
+  rt().dfree(w->d_bfp);
+  rt().dfree(w->d_bval);
+  rt().dfree(w->d_blcol);
+  rt().dfree(w->d_blrp);
+  rt().dfree(w->d_bnd);
+  rt().dfree(w->d_bstep);
   delete w;
+}
+
+template <class T, bool RC>
+void carp_run_blocks(const CarpWork<T>* w, int nvec, const T* sr, const T* si, const Mvec<T>* B, Mvec<T>* Xr,
+                     Mvec<T>* Xi, const T* omega)
+{
+  for (int c0 = 0; c0 < nvec; c0 += 32) {
+    const int nv = std::min(32, nvec - c0);
+    KaczBlockArgs<T> a;
+    memset(&a, 0, sizeof(a));
+    a.desc = w->d_desc; a.fp = w->d_bfp; a.val = w->d_bval; a.lcol = w->d_blcol;
+    a.lrp = w->d_blrp; a.nd = w->d_bnd; a.step = w->d_bstep;
+    a.nvec = nv;
+    a.max_fp = w->max_fp; a.max_rows = w->max_rows; a.max_nnz = w->max_nnz;
+    for (int j = 0; j < nv; j++) {
+      a.sig_r[j] = sr[c0 + j];
+      a.sig_i[j] = si ? si[c0 + j] : T(0);
+      a.omega[j] = omega[c0 + j];
+    }
+    a.b = B ? B->d() + c0 : nullptr;
+    a.ldb = B ? B->lda : 0;
+    a.xr = Xr->d() + c0;
+    a.ldxr = Xr->lda;
+    a.xi = Xi ? Xi->d() + c0 : nullptr;
+    a.ldxi = Xi ? Xi->lda : 0;
+    // TPR = nv rounded up to a power of two
+    const int TPR = nv <= 1 ? 1 : nv <= 2 ? 2 : nv <= 4 ? 4 : nv <= 8 ? 8 : nv <= 16 ? 16 : 32;
+    const CarpSmem L = carp_smem_layout(w->max_fp, w->max_rows, w->max_nnz, TPR, (int)sizeof(T), RC, a.b != nullptr);
+    PB_REQUIRE(L.total <= 227 * 1024, PB_NOT_IMPLEMENTED, "CARP block needs %d bytes of shared memory", L.total);
+    auto one = [&](int color, int dir) {
+      a.blk0 = w->h_bcolor_ptr[color];
+      const int64_t cnt = w->h_bcolor_ptr[color + 1] - a.blk0;
+      if (cnt <= 0) return;
+      a.dir = dir;
+#define PB_KB(TPRv)                                  \
+  {                                                  \
+    auto kern = k_kacz_blocks<T, TPRv, RC>;          \
+    set_smem(kern, L.total);                         \
+    kern<<<(unsigned)cnt, KB_NT, L.total, stream()>>>(a); \
+  }
+      if (TPR == 1) PB_KB(1)
+      else if (TPR == 2) PB_KB(2)
+      else if (TPR == 4) PB_KB(4)
+      else if (TPR == 8) PB_KB(8)
+      else if (TPR == 16) PB_KB(16)
+      else PB_KB(32)
+#undef PB_KB
+      PB_LAUNCH_CHECK();
+    };
+    // forward over the colours, the last colour forward and straight back,
+    // then backward over the others
+    const int C = w->nbcolors;
+    for (int c = 0; c < C - 1; c++) one(c, 1);
+    if (C > 0) one(C - 1, 3);
+    for (int c = C - 2; c >= 0; c--) one(c, 2);
+  }
 }
 
 template <class T, bool RC>
 void carp_run(const CarpWork<T>* w, int nvec, const T* sr, const T* si, const Mvec<T>* B,
               Mvec<T>* Xr, Mvec<T>* Xi, const T* omega)
 {
+  if (w->blocks) {
+    carp_run_blocks<T, RC>(w, nvec, sr, si, B, Xr, Xi, omega);
+    return;
+  }
   for (int c0 = 0; c0 < nvec; c0 += 32) {
     const int nv = std::min(32, nvec - c0);
     KaczArgs<T> a;

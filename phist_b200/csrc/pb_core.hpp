@@ -201,6 +201,10 @@ class Runtime {
   bool use_dmma = true;
   // batched CARP-CG replays its iteration as a CUDA graph (PHIST_B200_GRAPHS=0: plain launches)
   bool use_graphs = true;
+  // CARP sweeps over a block colouring with the footprint of X staged in
+  // shared memory (pb_carp_blocks.hpp); false: one launch per class of a
+  // distance-2 row colouring.  Read when the CARP work is set up.
+  bool carp_blocks = true;
 
   // statistics: kernel launches issued by this library (all lanes)
   std::atomic<uint64_t> launches{0};

@@ -45,6 +45,7 @@ void Runtime::init()
   if (const char* c = getenv("PHIST_B200_SELL_C")) sell_C = atoi(c);
   if (const char* s = getenv("PHIST_B200_SELL_SIGMA")) sell_sigma_default = atoll(s);
   if (const char* v = getenv("PHIST_B200_SPMV_PREFETCH")) spmv_pf = atoi(v) != 0;
+  if (const char* v = getenv("PHIST_B200_CARP_BLOCKS")) carp_blocks = atoi(v) != 0;
   noalloc_setup_current_device();
   inited_ = true;
 }
@@ -551,6 +552,7 @@ void phist_b200_set_option(const char* name, int value, int* iflag)
   if (o == "tma") rt().use_tma = value != 0;
   else if (o == "dmma") rt().use_dmma = value != 0;
   else if (o == "graphs") rt().use_graphs = value != 0;
+  else if (o == "carp_blocks") rt().carp_blocks = value != 0;
   else PB_REQUIRE(false, PB_INVALID_INPUT, "unknown option '%s'", name);
   PB_API_END(iflag);
 }

@@ -1,11 +1,15 @@
 """CARP sweeps on the GPU (carp_setup / carp_sweep / carp_destroy).
 
-The GPU sweep runs colour class by colour class of a distance-2 colouring;
-it must equal the oracle's sequential Kaczmarz sweep over the same row order
-(kacz_sub_def.h update formulae) to rounding, the colouring must be a valid
-distance-2 colouring, repeated sweeps must be bitwise reproducible (the
-reference's CarpTest checks repeatability, CarpTest_def.hpp:579-611), and
-sweeps must drive the residual of (A - sigma I) x = b down.
+Two layouts: the default block-coloured sweep (row blocks with their X
+footprint staged in shared memory, one launch per block colour) and the
+row-colour sweep (one launch per class of a distance-2 colouring; option
+carp_blocks = 0).  Either must equal the oracle's sequential Kaczmarz sweep
+over the row order the library reports (kacz_sub_def.h update formulae) to
+rounding, the segments of that order must be distance-2 independent sets,
+repeated sweeps must be bitwise reproducible (the reference's CarpTest checks
+repeatability, CarpTest_def.hpp:579-611), and sweeps must drive the residual
+of (A - sigma I) x = b down.  The block sweep is also checked at the
+benchmarked size (honeycomb 1024 x 1024 x 2 sites, 8 shifts).
 """
 import ctypes as ct
 
@@ -15,6 +19,14 @@ import pytest
 from conftest import relerr
 
 pytestmark = pytest.mark.gpu
+
+
+@pytest.fixture(params=[1, 0], ids=["blocks", "rowcolour"])
+def layout(request, session):
+    from phist_b200 import kernels as K
+    K.chk(K.phist_b200_set_option, b"carp_blocks", request.param)
+    yield request.param
+    K.chk(K.phist_b200_set_option, b"carp_blocks", 1)
 
 
 def _setup(A, shifts, dtype=np.float64):
@@ -51,7 +63,7 @@ def _order(work, n):
 @pytest.mark.parametrize("prob,nvec", [("sprandn388", 1), ("sprandn388", 4), ("symmMat20", 3),
                                        ("spshift388", 8), ("jadaTestMat512", 2),
                                        ("sprandn_nodiag388", 4), ("spshift25", 1)])
-def test_carp_sweep_vs_oracle(session, oracle, testmats, prob, nvec):
+def test_carp_sweep_vs_oracle(session, layout, oracle, testmats, prob, nvec):
     from phist_b200 import kernels as K
     from phist_b200.objects import Mvec, SparseMat
     rp, c, v, shape = testmats(prob)
@@ -119,7 +131,7 @@ def test_carp_converges_honeycomb(session, oracle):
         o.delete()
 
 
-def test_carp_rc_reduces_to_real(session, oracle, testmats):
+def test_carp_rc_reduces_to_real(session, layout, oracle, testmats):
     """complex-shift variant with zero imaginary parts equals the real sweep"""
     from phist_b200 import kernels as K
     from phist_b200.objects import Mvec, SparseMat
@@ -145,6 +157,70 @@ def test_carp_rc_reduces_to_real(session, oracle, testmats):
     assert np.abs(Xi.get()).max() == 0.0
     K.chk(K.phist_Dcarp_destroy, A.h, work)
     for o in (Xr, Xi, B, A):
+        o.delete()
+
+
+@pytest.mark.parametrize("nvec", [8, 32])
+def test_carp_block_sweep_benchmark_size(session, oracle, nvec):
+    """the benchmarked matrix: honeycomb 1024 x 1024 cells, 2 sites each
+    (n = 2,097,152), block layout, against the oracle's sequential sweep in
+    the reported order"""
+    import os
+
+    from phist_b200 import generators as G
+    from phist_b200 import kernels as K
+    from phist_b200.objects import Mvec, SparseMat
+    oracle.set_threads(os.cpu_count() or 1)
+    rp, c, v = G.honeycomb(1024, 1024, 1)
+    n = len(rp) - 1
+    A = SparseMat.from_crs(rp, c, v)
+    rng = np.random.default_rng(nvec)
+    shifts = rng.uniform(-2, 2, nvec)
+    omega = np.full(nvec, 1.2)
+    x0 = rng.uniform(-1, 1, (n, nvec))
+    b = rng.uniform(-1, 1, (n, nvec))
+    work, sh = _setup(A, shifts)
+    rows, cp = _order(work, n)
+    assert len(cp) - 1 <= 64  # block colours x steps: few segments
+    X = Mvec(A.row_map, nvec).set(x0)
+    B = Mvec(A.row_map, nvec).set(b)
+    K.chk(K.phist_Dcarp_sweep, A.h, K.sptr(sh, np.float64), B.h, X.h, work, K.sptr(omega, np.float64))
+    ref = oracle.carp_sweep(rp, c, v, shifts, b, x0, omega, order=rows)
+    assert relerr(X.get(), ref) < 1e-13
+    K.chk(K.phist_Dcarp_destroy, A.h, work)
+    for o in (X, B, A):
+        o.delete()
+
+
+def test_carp_sweep_strided_views(session, layout, oracle):
+    """X and B as column views of wider mvecs (leading dimension > nvec)"""
+    from phist_b200 import generators as G
+    from phist_b200 import kernels as K
+    from phist_b200.objects import Mvec, SparseMat
+    rp, c, v = G.honeycomb(30, 20, 2)
+    n = len(rp) - 1
+    A = SparseMat.from_crs(rp, c, v)
+    nvec = 3
+    rng = np.random.default_rng(9)
+    shifts = rng.uniform(-1, 1, nvec)
+    omega = np.ones(nvec)
+    x0 = rng.uniform(-1, 1, (n, nvec))
+    b = rng.uniform(-1, 1, (n, nvec))
+    work, sh = _setup(A, shifts)
+    rows, _ = _order(work, n)
+    Xw = Mvec(A.row_map, 7).set(rng.uniform(-1, 1, (n, 7)))
+    Bw = Mvec(A.row_map, 5).set(rng.uniform(-1, 1, (n, 5)))
+    X = Xw.view(2, 4)
+    B = Bw.view(1, 3)
+    X.set(x0)
+    B.set(b)
+    K.chk(K.phist_Dcarp_sweep, A.h, K.sptr(sh, np.float64), B.h, X.h, work, K.sptr(omega, np.float64))
+    ref = oracle.carp_sweep(rp, c, v, shifts, b, x0, omega, order=rows)
+    assert relerr(X.get(), ref) < 1e-13
+    full = Xw.get()
+    assert relerr(full[:, 2:5], ref) < 1e-13
+    K.chk(K.phist_Dcarp_destroy, A.h, work)
+    for o in (X, B, Xw, Bw, A):
         o.delete()
 
 
