@@ -1472,17 +1472,19 @@ RowGemmArgs<T> rowgemm_args()
 // ======================================================================
 // CARP
 // ======================================================================
-// Block-coloured layout (pb_carp_blocks.hpp): blocks of at most 128 rows
-// whose footprint has at most 256 rows of X and whose pattern at most 2048
-// entries.  False when the matrix has rows too long for that, or a block
-// needs more than 64 steps; the caller then uses the row colouring.
+// Block-coloured layout (pb_carp_blocks.hpp): blocks of at most R rows
+// (runtime carp_block_rows, 128 by default) whose footprint has at most 2R
+// rows of X and whose pattern at most 16R entries.  False when the matrix has
+// rows too long for that, or a block needs more than 64 steps; the caller
+// then uses the row colouring.
 template <class T>
 bool carp_build_blocks(const SparseMat<T>* A, const std::vector<int64_t>& prp, const std::vector<int32_t>& pcol,
                        CarpWork<T>* w)
 {
   const int64_t n = A->nrows;
   CarpBlocks B;
-  if (!carp_block_partition(n, prp, pcol, 128, 256, 2048, B)) return false;
+  const int R = rt().carp_block_rows;
+  if (!carp_block_partition(n, prp, pcol, R, 2 * R, 16 * R, B)) return false;
   if (!carp_block_color(n, prp, pcol, B)) return false;
   CarpBlockLayout<T> L;
   carp_block_layout<T>(B, n, A->h_row_ptr.data(), A->h_col.data(), A->h_val.data(), L);
@@ -1491,17 +1493,24 @@ bool carp_build_blocks(const SparseMat<T>* A, const std::vector<int64_t>& prp, c
   w->h_bcolor_ptr = B.color_ptr;
   w->max_fp = B.max_fp;
   w->max_rows = B.max_rows;
-  w->max_nnz = L.max_nnz;
+  w->seg_stride = L.stride;
+  {
+    // rows without a repeated column let the sweep update gathered values
+    std::vector<int64_t> seen(n, -1);
+    w->distinct = true;
+    for (int64_t i = 0; i < n && w->distinct; i++)
+      for (int64_t p = A->h_row_ptr[i]; p < A->h_row_ptr[i + 1]; p++) {
+        if (seen[A->h_col[p]] == i) {
+          w->distinct = false;
+          break;
+        }
+        seen[A->h_col[p]] = i;
+      }
+  }
   w->h_rows = B.seq_rows;
   w->h_color_ptr = B.seq_ptr;
   w->ncolors = (int)B.seq_ptr.size() - 1;
-  w->d_desc = (CarpBlockDesc*)upload_vec(L.desc);
-  w->d_bfp = (int32_t*)upload_vec(L.fp);
-  w->d_bval = (T*)upload_vec(L.val);
-  w->d_blcol = (uint16_t*)upload_vec(L.lcol);
-  w->d_blrp = (uint16_t*)upload_vec(L.lrp);
-  w->d_bnd = (T*)upload_vec(L.nd);
-  w->d_bstep = (uint16_t*)upload_vec(L.step);
+  w->d_bseg = (unsigned char*)upload_vec(L.seg);
   return true;
 }
 
@@ -1584,13 +1593,7 @@ void carp_free(CarpWork<T>* w)
   rt().dfree(w->d_val);
   rt().dfree(w->d_nrm);
   rt().dfree(w->d_diag);
-  rt().dfree(w->d_desc);
-  rt().dfree(w->d_bfp);
-  rt().dfree(w->d_bval);
-  rt().dfree(w->d_blcol);
-  rt().dfree(w->d_blrp);
-  rt().dfree(w->d_bnd);
-  rt().dfree(w->d_bstep);
+  rt().dfree(w->d_bseg);
   delete w;
 }
 
@@ -1602,10 +1605,10 @@ void carp_run_blocks(const CarpWork<T>* w, int nvec, const T* sr, const T* si, c
     const int nv = std::min(32, nvec - c0);
     KaczBlockArgs<T> a;
     memset(&a, 0, sizeof(a));
-    a.desc = w->d_desc; a.fp = w->d_bfp; a.val = w->d_bval; a.lcol = w->d_blcol;
-    a.lrp = w->d_blrp; a.nd = w->d_bnd; a.step = w->d_bstep;
+    a.seg = w->d_bseg;
     a.nvec = nv;
-    a.max_fp = w->max_fp; a.max_rows = w->max_rows; a.max_nnz = w->max_nnz;
+    a.max_fp = w->max_fp; a.max_rows = w->max_rows; a.seg_stride = w->seg_stride;
+    a.distinct = w->distinct ? 1 : 0;
     for (int j = 0; j < nv; j++) {
       a.sig_r[j] = sr[c0 + j];
       a.sig_i[j] = si ? si[c0 + j] : T(0);
@@ -1619,18 +1622,42 @@ void carp_run_blocks(const CarpWork<T>* w, int nvec, const T* sr, const T* si, c
     a.ldxi = Xi ? Xi->lda : 0;
     // TPR = nv rounded up to a power of two
     const int TPR = nv <= 1 ? 1 : nv <= 2 ? 2 : nv <= 4 ? 4 : nv <= 8 ? 8 : nv <= 16 ? 16 : 32;
-    const CarpSmem L = carp_smem_layout(w->max_fp, w->max_rows, w->max_nnz, TPR, (int)sizeof(T), RC, a.b != nullptr);
+    // X and B copied in 16-byte pieces where every row of both starts on a
+    // 16-byte boundary and the columns fill whole pieces
+    constexpr int WV = 16 / (int)sizeof(T);
+    auto al16 = [](const void* p) { return ((uintptr_t)p & 15) == 0; };
+    const bool wide = nv % WV == 0 && al16(a.xr) && a.ldxr % WV == 0 && (!RC || (al16(a.xi) && a.ldxi % WV == 0)) &&
+                      (!a.b || (al16(a.b) && a.ldb % WV == 0));
+    const CarpSmem L =
+        carp_smem_layout(w->max_fp, w->max_rows, w->seg_stride, TPR, (int)sizeof(T), RC, a.b != nullptr);
     PB_REQUIRE(L.total <= 227 * 1024, PB_NOT_IMPLEMENTED, "CARP block needs %d bytes of shared memory", L.total);
     auto one = [&](int color, int dir) {
       a.blk0 = w->h_bcolor_ptr[color];
       const int64_t cnt = w->h_bcolor_ptr[color + 1] - a.blk0;
       if (cnt <= 0) return;
       a.dir = dir;
-#define PB_KB(TPRv)                                  \
-  {                                                  \
-    auto kern = k_kacz_blocks<T, TPRv, RC>;          \
-    set_smem(kern, L.total);                         \
-    kern<<<(unsigned)cnt, KB_NT, L.total, stream()>>>(a); \
+      // one thread block per row block; with a programmatic dependency on
+      // the previous launch in the stream (its blocks copy their segments
+      // during that launch's tail)
+      auto go = [&](auto kern) {
+        set_smem(kern, L.total);
+        cudaLaunchConfig_t cfg;
+        memset(&cfg, 0, sizeof(cfg));
+        cfg.gridDim = dim3((unsigned)cnt);
+        cfg.blockDim = dim3(KB_NT);
+        cfg.dynamicSmemBytes = L.total;
+        cfg.stream = stream();
+        cudaLaunchAttribute attr[1];
+        attr[0].id = cudaLaunchAttributeProgrammaticStreamSerialization;
+        attr[0].val.programmaticStreamSerializationAllowed = 1;
+        cfg.attrs = attr;
+        cfg.numAttrs = rt().carp_pdl ? 1 : 0;
+        PB_CUDA(cudaLaunchKernelEx(&cfg, kern, a));
+      };
+#define PB_KB(TPRv)                                              \
+  {                                                              \
+    if (wide) go(k_kacz_blocks<T, TPRv, RC, KB_NT, WV>);        \
+    else go(k_kacz_blocks<T, TPRv, RC, KB_NT, 1>);              \
   }
       if (TPR == 1) PB_KB(1)
       else if (TPR == 2) PB_KB(2)

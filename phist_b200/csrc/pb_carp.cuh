@@ -49,14 +49,9 @@ struct CarpWork {
   bool blocks = false;
   int nbcolors = 0;
   std::vector<int64_t> h_bcolor_ptr;  // blocks [bcolor_ptr[c], bcolor_ptr[c+1]) have colour c
-  int max_fp = 0, max_rows = 0, max_nnz = 0;
-  CarpBlockDesc* d_desc = nullptr;
-  int32_t* d_bfp = nullptr;
-  T* d_bval = nullptr;
-  uint16_t* d_blcol = nullptr;
-  uint16_t* d_blrp = nullptr;
-  T* d_bnd = nullptr;
-  uint16_t* d_bstep = nullptr;
+  int max_fp = 0, max_rows = 0, seg_stride = 0;
+  bool distinct = false;               // no row holds a column twice
+  unsigned char* d_bseg = nullptr;     // block segments, seg_stride bytes apart
 };
 
 template <class T>
@@ -135,17 +130,12 @@ __global__ void __launch_bounds__(256) k_kacz_color_cols(KaczArgs<T> a)
 
 template <class T>
 struct KaczBlockArgs {
-  const CarpBlockDesc* __restrict__ desc;
-  const int32_t* __restrict__ fp;
-  const T* __restrict__ val;
-  const uint16_t* __restrict__ lcol;
-  const uint16_t* __restrict__ lrp;
-  const T* __restrict__ nd;
-  const uint16_t* __restrict__ step;
-  int64_t blk0;   // first block of this launch; thread block k takes block blk0 + k
-  int dir;        // 1 forward, 2 backward, 3 forward then backward
+  const unsigned char* __restrict__ seg;   // segment b at b * seg_stride
+  int64_t blk0;          // first block of the launch; thread block k takes block blk0 + k
+  int dir;              // 1 forward, 2 backward, 3 forward then backward
   int nvec;
-  int max_fp, max_rows, max_nnz;
+  int max_fp, max_rows, seg_stride;
+  int distinct;         // no row holds a column twice
   T sig_r[32];
   T sig_i[32];
   T omega[32];
@@ -154,158 +144,310 @@ struct KaczBlockArgs {
   T* xi; int64_t ldxi;       // rc variant only
 };
 
-constexpr int KB_NT = 256;
+constexpr int KB_NT = 128;  // threads per block of the block sweep
 
-template <class T>
-__device__ __forceinline__ void cp_async_elem(T* s, const T* g)
+// cp.async of BYTES (4, 8 or 16) from global to shared memory
+template <int BYTES>
+__device__ __forceinline__ void cp_async_n(void* s, const void* g)
 {
   const unsigned sa = (unsigned)__cvta_generic_to_shared(s);
-  if constexpr (sizeof(T) == 8)
-    asm volatile("cp.async.ca.shared.global [%0], [%1], 8;\n" ::"r"(sa), "l"(g) : "memory");
+  if constexpr (BYTES == 16)
+    asm volatile("cp.async.cg.shared.global [%0], [%1], 16;\n" ::"r"(sa), "l"(g) : "memory");
   else
-    asm volatile("cp.async.ca.shared.global [%0], [%1], 4;\n" ::"r"(sa), "l"(g) : "memory");
+    asm volatile("cp.async.ca.shared.global [%0], [%1], %2;\n" ::"r"(sa), "l"(g), "n"(BYTES) : "memory");
 }
 
-// One thread block per row block.  (1) cp.async the block's segments (matrix
-// entries with footprint-local columns, entry offsets, norms and diagonals,
-// footprint rows, step starts), the footprint rows of X and the rows of B
-// into shared memory; (2) run the steps, forward and/or backward: in a step
-// thread (r, j), TPR threads per row, projects row r of the step for column
-// j with the update formulae above, all in shared memory, the rows of one
-// step touching disjoint footprint slots; a barrier separates the steps;
-// (3) write the footprint rows of X back.  Blocks of one launch have
-// disjoint footprints.
-template <class T, int TPR, bool RC>
-__global__ void __launch_bounds__(KB_NT) k_kacz_blocks(KaczBlockArgs<T> a)
+// CPT consecutive elements of T (CPT * sizeof(T) <= 16, aligned)
+template <class T, int CPT>
+struct CarpVec {
+  T v[CPT];
+};
+template <class T, int CPT>
+__device__ __forceinline__ CarpVec<T, CPT> cv_ld(const T* p)
 {
+  CarpVec<T, CPT> r;
+  if constexpr (CPT * sizeof(T) == 16) {
+    const double2 q = *(const double2*)p;
+    memcpy(&r, &q, 16);
+  } else if constexpr (CPT * sizeof(T) == 8) {
+    const double q = *(const double*)p;
+    memcpy(&r, &q, 8);
+  } else {
+    r.v[0] = p[0];
+  }
+  return r;
+}
+template <class T, int CPT>
+__device__ __forceinline__ void cv_st(T* p, const CarpVec<T, CPT>& r)
+{
+  if constexpr (CPT * sizeof(T) == 16) {
+    double2 q;
+    memcpy(&q, &r, 16);
+    *(double2*)p = q;
+  } else if constexpr (CPT * sizeof(T) == 8) {
+    double q;
+    memcpy(&q, &r, 8);
+    *(double*)p = q;
+  } else {
+    p[0] = r.v[0];
+  }
+}
+
+// One thread block per row block of one colour (blocks blk0 + blockIdx.x;
+// the blocks of a launch have disjoint footprints).  Two copy stages
+// precede the steps:
+//   H: cp.async the head of the block's segment (header, footprint rows)
+//   X: cp.async the rest of the segment (entries with footprint-local
+//      columns, norms and diagonals, entry offsets, step starts), the
+//      footprint rows of X and the block's rows of B
+// then the steps, forward and/or backward, and X written back.  Many
+// thread blocks per SM overlap one another's copies and steps.
+//
+// X rows are copied in pieces of W elements (16 bytes when the caller's
+// alignment allows, else one element).  In a step, thread (r, q) projects
+// row r of the step for the CPT columns q*CPT.. (TPR/CPT threads per row):
+// the row's entries are read once for its CPT columns and X is read and
+// written CPT columns at a time; each column follows the update formulae
+// above in the same order.  Rows of one step touch disjoint footprint slots
+// and a barrier separates the steps.
+template <class T, int TPR, bool RC, int NT, int W>
+__global__ void __launch_bounds__(NT) k_kacz_blocks(KaczBlockArgs<T> a)
+{
+  constexpr int CPT = (TPR >= 16 / (int)sizeof(T)) ? 16 / (int)sizeof(T) : TPR;  // columns per thread
+  constexpr int TPRC = TPR / CPT;                                                  // threads per row
+  constexpr int RE = 4;  // entries of a row held in registers
+  using V = CarpVec<T, CPT>;
   extern __shared__ __align__(16) unsigned char smem[];
-  const CarpSmem L = carp_smem_layout(a.max_fp, a.max_rows, a.max_nnz, TPR, (int)sizeof(T), RC, a.b != nullptr);
-  T* xs = (T*)(smem + L.xs);
-  T* xis = (T*)(smem + L.xis);
-  T* bs = (T*)(smem + L.bs);
-  T* vs = (T*)(smem + L.val);
-  T* nds = (T*)(smem + L.nd);
-  int32_t* fps = (int32_t*)(smem + L.fp);
-  uint16_t* lcs = (uint16_t*)(smem + L.lcol);
-  uint16_t* lrs = (uint16_t*)(smem + L.lrp);
-  uint16_t* sts = (uint16_t*)(smem + L.step);
+  const CarpSmem L = carp_smem_layout(a.max_fp, a.max_rows, a.seg_stride, TPR, (int)sizeof(T), RC, a.b != nullptr);
+  const int head = carp_seg_head(a.max_fp);
   const int tid = threadIdx.x;
   const int nv = a.nvec;
-  const CarpBlockDesc d = a.desc[a.blk0 + blockIdx.x];
+  unsigned char* mb = smem + L.mbase;   // the block's segment
+  unsigned char* xb = smem + L.xbase;   // its X and B rows
+  const unsigned char* gseg = a.seg + (a.blk0 + blockIdx.x) * a.seg_stride;
+
+  // the next launch may start its thread blocks as this one's finish: they
+  // copy their segments (read-only) and then wait for this grid to complete
+  // before they touch X or B (griddepcontrol.wait below; both are no-ops
+  // without a programmatic dependency)
+  asm volatile("griddepcontrol.launch_dependents;" ::: "memory");
+  // H: header and footprint rows
+  for (int c = tid; c < head / 16; c += NT) cp_async_n<16>(mb + 16 * c, gseg + 16 * c);
+  cp_async_commit();
+  cp_async_wait<0>();
+  __syncthreads();
+  // X: the rest of the segment, footprint rows of X (own rows first), rows
+  // of B
   {
-    // 16-byte chunks of the block's segments
-    const int nval = carp_r8(d.nnz) * (int)sizeof(T) / 16;
-    const int nlc = carp_r8(d.nnz) * 2 / 16;
-    const int nlr = carp_r8(d.nrows + 1) * 2 / 16;
-    const int nnd = carp_r8(d.nrows) * 2 * (int)sizeof(T) / 16;
-    const int nfp = ((d.nfp + 3) & ~3) * 4 / 16;
-    const int nst = carp_r8(d.nsteps + 1) * 2 / 16;
-    const int tot = nval + nlc + nlr + nnd + nfp + nst;
-    for (int c = tid; c < tot; c += KB_NT) {
-      int k = c;
-      const char* g;
-      char* sp;
-      if (k < nval) {
-        g = (const char*)(a.val + d.ent);
-        sp = (char*)vs;
-      } else if ((k -= nval) < nlc) {
-        g = (const char*)(a.lcol + d.ent);
-        sp = (char*)lcs;
-      } else if ((k -= nlc) < nlr) {
-        g = (const char*)(a.lrp + d.row);
-        sp = (char*)lrs;
-      } else if ((k -= nlr) < nnd) {
-        g = (const char*)(a.nd + 2 * d.row);
-        sp = (char*)nds;
-      } else if ((k -= nnd) < nfp) {
-        g = (const char*)(a.fp + d.fp);
-        sp = (char*)fps;
-      } else {
-        k -= nfp;
-        g = (const char*)(a.step + d.step);
-        sp = (char*)sts;
-      }
-      cp_async16(sp + 16 * k, g + 16 * k, true);
-    }
-    // footprint rows of X (own rows first) and the block's rows of B
-    for (int e = tid; e < d.nfp * TPR; e += KB_NT) {
-      const int u = e / TPR, j = e % TPR;
+    const int32_t* hdr = (const int32_t*)mb;
+    const int nrows = hdr[0], nfp = hdr[1];
+    const int bytes = carp_seg(hdr[0], hdr[1], hdr[2], hdr[3], (int)sizeof(T)).bytes;
+    for (int c = head / 16 + tid; c < bytes / 16; c += NT) cp_async_n<16>(mb + 16 * c, gseg + 16 * c);
+    asm volatile("griddepcontrol.wait;" ::: "memory");
+    const int32_t* fps = (const int32_t*)(mb + 16);
+    T* xs = (T*)(xb + L.xs);
+    T* xis = (T*)(xb + L.xis);
+    T* bs = (T*)(xb + L.bs);
+    constexpr int PW = TPR / W;  // pieces per footprint row
+    for (int e = tid; e < nfp * PW; e += NT) {
+      const int u = e / PW, j = (e % PW) * W;
       if (j < nv) {
-        const int64_t g = a.fp[d.fp + u];
-        cp_async_elem(xs + e, a.xr + g * a.ldxr + j);
-        if (RC) cp_async_elem(xis + e, a.xi + g * a.ldxi + j);
+        const int64_t g = fps[u];
+        cp_async_n<W * sizeof(T)>(xs + u * TPR + j, a.xr + g * a.ldxr + j);
+        if (RC) cp_async_n<W * sizeof(T)>(xis + u * TPR + j, a.xi + g * a.ldxi + j);
       }
     }
     if (a.b) {
-      for (int e = tid; e < d.nrows * TPR; e += KB_NT) {
-        const int r = e / TPR, j = e % TPR;
-        if (j < nv) cp_async_elem(bs + e, a.b + (int64_t)a.fp[d.fp + r] * a.ldb + j);
+      for (int e = tid; e < nrows * PW; e += NT) {
+        const int r = e / PW, j = (e % PW) * W;
+        if (j < nv) cp_async_n<W * sizeof(T)>(bs + r * TPR + j, a.b + (int64_t)fps[r] * a.ldb + j);
       }
     }
     cp_async_commit();
     cp_async_wait<0>();
     __syncthreads();
   }
-  auto project = [&](int r, int j) {
-    const T sr = a.sig_r[j];
-    const T si = RC ? a.sig_i[j] : T(0);
-    const int e0 = lrs[r], e1 = lrs[r + 1];
-    T tr, ti = T(0);
-    {
-      const T x0 = xs[r * TPR + j];
-      if (RC) {
-        const T y0 = xis[r * TPR + j];
-        tr = -sr * x0 + si * y0;
-        ti = -si * x0 - sr * y0;
-      } else {
-        tr = -sr * x0;
+
+  // the steps and the write-back
+  {
+    const int32_t* hdr = (const int32_t*)mb;
+    const CarpSeg sg = carp_seg(hdr[0], hdr[1], hdr[2], hdr[3], (int)sizeof(T));
+    const int32_t* fps = (const int32_t*)(mb + sg.fp);
+    const T* vs = (const T*)(mb + sg.val);
+    const T* nds = (const T*)(mb + sg.nd);
+    const uint16_t* lcs = (const uint16_t*)(mb + sg.lcol);
+    const uint16_t* lrs = (const uint16_t*)(mb + sg.lrp);
+    const uint16_t* sts = (const uint16_t*)(mb + sg.step);
+    T* xs = (T*)(xb + L.xs);
+    T* xis = (T*)(xb + L.xis);
+    const T* bs = (const T*)(xb + L.bs);
+
+    auto project = [&](int r, int j0) {
+      const int e0 = lrs[r], e1 = lrs[r + 1];
+      const T nrm = nds[2 * r], dg = nds[2 * r + 1];
+      // the scaling does not depend on X: formed while the gathers are out
+      T f[CPT], sr[CPT], si[CPT];
+#pragma unroll
+      for (int k = 0; k < CPT; k++) {
+        sr[k] = a.sig_r[j0 + k];
+        si[k] = RC ? a.sig_i[j0 + k] : T(0);
+        T rn = nrm - T(2) * dg * sr[k] + sr[k] * sr[k];
+        if (RC) rn += si[k] * si[k];
+        if (rn == T(0)) rn = T(1);
+        f[k] = a.omega[j0 + k] / rn;
       }
-    }
-    for (int p = e0; p < e1; p++) {
-      const T v = vs[p];
-      const int c = lcs[p];
-      tr += v * xs[c * TPR + j];
-      if (RC) ti += v * xis[c * TPR + j];
-    }
-    if (a.b) tr -= bs[r * TPR + j];
-    const T nrm = nds[2 * r], dg = nds[2 * r + 1];
-    T rn = nrm - T(2) * dg * sr + sr * sr;
-    if (RC) rn += si * si;
-    if (rn == T(0)) rn = T(1);
-    const T f = a.omega[j] / rn;
-    tr *= f;
-    if (RC) {
-      ti *= f;
-      xs[r * TPR + j] += tr * sr + ti * si;
-      xis[r * TPR + j] += ti * sr - tr * si;
-    } else {
-      xs[r * TPR + j] += tr * sr;
-    }
-    for (int p = e0; p < e1; p++) {
-      const T v = vs[p];
-      const int c = lcs[p];
-      xs[c * TPR + j] -= tr * v;
-      if (RC) xis[c * TPR + j] -= ti * v;
-    }
-  };
-  auto run_step = [&](int s) {
-    const int lo = sts[s], hi = sts[s + 1];
-    for (int e = tid; e < (hi - lo) * TPR; e += KB_NT) {
-      const int j = e % TPR;
-      if (j < nv) project(lo + e / TPR, j);
-    }
-    __syncthreads();
-  };
-  if (a.dir & 1)
-    for (int s = 0; s < d.nsteps; s++) run_step(s);
-  if (a.dir & 2)
-    for (int s = d.nsteps - 1; s >= 0; s--) run_step(s);
-  for (int e = tid; e < d.nfp * TPR; e += KB_NT) {
-    const int u = e / TPR, j = e % TPR;
-    if (j < nv) {
-      const int64_t g = fps[u];
-      a.xr[g * a.ldxr + j] = xs[e];
-      if (RC) a.xi[g * a.ldxi + j] = xis[e];
+      T tr[CPT], ti[CPT];
+      const V x0 = cv_ld<T, CPT>(xs + r * TPR + j0);
+      V y0;
+      if (RC) y0 = cv_ld<T, CPT>(xis + r * TPR + j0);
+#pragma unroll
+      for (int k = 0; k < CPT; k++) {
+        if (RC) {
+          tr[k] = -sr[k] * x0.v[k] + si[k] * y0.v[k];
+          ti[k] = -si[k] * x0.v[k] - sr[k] * y0.v[k];
+        } else {
+          tr[k] = -sr[k] * x0.v[k];
+          ti[k] = T(0);
+        }
+      }
+      T v[RE];
+      int c[RE];
+#pragma unroll
+      for (int q = 0; q < RE; q++) {
+        const bool in = e0 + q < e1;
+        v[q] = in ? vs[e0 + q] : T(0);
+        c[q] = in ? (int)lcs[e0 + q] : r;
+      }
+      V xg[RE], yg[RE];
+#pragma unroll
+      for (int q = 0; q < RE; q++) {
+        xg[q] = cv_ld<T, CPT>(xs + c[q] * TPR + j0);
+        if (RC) yg[q] = cv_ld<T, CPT>(xis + c[q] * TPR + j0);
+      }
+#pragma unroll
+      for (int q = 0; q < RE; q++)
+        if (e0 + q < e1) {
+#pragma unroll
+          for (int k = 0; k < CPT; k++) {
+            tr[k] += v[q] * xg[q].v[k];
+            if (RC) ti[k] += v[q] * yg[q].v[k];
+          }
+        }
+      for (int p = e0 + RE; p < e1; p++) {
+        const T vv = vs[p];
+        const int cc = lcs[p];
+        const V xx = cv_ld<T, CPT>(xs + cc * TPR + j0);
+        V yy;
+        if (RC) yy = cv_ld<T, CPT>(xis + cc * TPR + j0);
+#pragma unroll
+        for (int k = 0; k < CPT; k++) {
+          tr[k] += vv * xx.v[k];
+          if (RC) ti[k] += vv * yy.v[k];
+        }
+      }
+      if (a.b) {
+        const V bb = cv_ld<T, CPT>(bs + r * TPR + j0);
+#pragma unroll
+        for (int k = 0; k < CPT; k++) tr[k] -= bb.v[k];
+      }
+#pragma unroll
+      for (int k = 0; k < CPT; k++) {
+        tr[k] *= f[k];
+        if (RC) ti[k] *= f[k];
+      }
+      if (a.distinct && e1 - e0 <= RE) {
+        // the row's columns are distinct and its entries are in registers:
+        // update the values gathered above (no other thread of the step
+        // touches these slots), x_i first with the shift term, then every
+        // entry in order (the diagonal one continuing from x_i), and store
+        // each slot once
+        V xo = x0, yo = y0;
+#pragma unroll
+        for (int k = 0; k < CPT; k++) {
+          if (RC) {
+            xo.v[k] += tr[k] * sr[k] + ti[k] * si[k];
+            yo.v[k] += ti[k] * sr[k] - tr[k] * si[k];
+          } else {
+            xo.v[k] += tr[k] * sr[k];
+          }
+        }
+#pragma unroll
+        for (int q = 0; q < RE; q++)
+          if (e0 + q < e1) {
+            const bool own = c[q] == r;
+            V t = own ? xo : xg[q];
+            V u;
+            if (RC) u = own ? yo : yg[q];
+#pragma unroll
+            for (int k = 0; k < CPT; k++) {
+              t.v[k] -= tr[k] * v[q];
+              if (RC) u.v[k] -= ti[k] * v[q];
+            }
+            if (own) {
+              xo = t;
+              if (RC) yo = u;
+            } else {
+              cv_st<T, CPT>(xs + c[q] * TPR + j0, t);
+              if (RC) cv_st<T, CPT>(xis + c[q] * TPR + j0, u);
+            }
+          }
+        cv_st<T, CPT>(xs + r * TPR + j0, xo);
+        if (RC) cv_st<T, CPT>(xis + r * TPR + j0, yo);
+        return;
+      }
+      {
+        V x0 = cv_ld<T, CPT>(xs + r * TPR + j0);
+        if (RC) {
+          V y0 = cv_ld<T, CPT>(xis + r * TPR + j0);
+#pragma unroll
+          for (int k = 0; k < CPT; k++) {
+            x0.v[k] += tr[k] * sr[k] + ti[k] * si[k];
+            y0.v[k] += ti[k] * sr[k] - tr[k] * si[k];
+          }
+          cv_st<T, CPT>(xis + r * TPR + j0, y0);
+        } else {
+#pragma unroll
+          for (int k = 0; k < CPT; k++) x0.v[k] += tr[k] * sr[k];
+        }
+        cv_st<T, CPT>(xs + r * TPR + j0, x0);
+      }
+      auto scatter = [&](int cc, T vv) {
+        V xx = cv_ld<T, CPT>(xs + cc * TPR + j0);
+#pragma unroll
+        for (int k = 0; k < CPT; k++) xx.v[k] -= tr[k] * vv;
+        cv_st<T, CPT>(xs + cc * TPR + j0, xx);
+        if (RC) {
+          V yy = cv_ld<T, CPT>(xis + cc * TPR + j0);
+#pragma unroll
+          for (int k = 0; k < CPT; k++) yy.v[k] -= ti[k] * vv;
+          cv_st<T, CPT>(xis + cc * TPR + j0, yy);
+        }
+      };
+#pragma unroll
+      for (int q = 0; q < RE; q++)
+        if (e0 + q < e1) scatter(c[q], v[q]);
+      for (int p = e0 + RE; p < e1; p++) scatter(lcs[p], vs[p]);
+    };
+    auto run_step = [&](int st) {
+      const int lo = sts[st], hi = sts[st + 1];
+      for (int e = tid; e < (hi - lo) * TPRC; e += NT) {
+        const int j0 = (e % TPRC) * CPT;
+        if (j0 < nv) project(lo + e / TPRC, j0);
+      }
+      __syncthreads();
+    };
+    if (a.dir & 1)
+      for (int st = 0; st < sg.nsteps; st++) run_step(st);
+    if (a.dir & 2)
+      for (int st = sg.nsteps - 1; st >= 0; st--) run_step(st);
+    constexpr int PW = TPR / W;
+    for (int e = tid; e < sg.nfp * PW; e += NT) {
+      const int u = e / PW, j = (e % PW) * W;
+      if (j < nv) {
+        const int64_t g = fps[u];
+        cv_st<T, W>(a.xr + g * a.ldxr + j, cv_ld<T, W>(xs + u * TPR + j));
+        if (RC) cv_st<T, W>(a.xi + g * a.ldxi + j, cv_ld<T, W>(xis + u * TPR + j));
+      }
     }
   }
 }

@@ -24,6 +24,7 @@
 #pragma once
 #include <algorithm>
 #include <cstdint>
+#include <cstring>
 #include <vector>
 
 #ifdef __CUDACC__
@@ -34,26 +35,60 @@
 
 namespace pb {
 
-// one row block of the block-coloured sweep; every offset is a multiple of
-// 16 bytes in its array and every per-block segment is padded to 16 bytes,
-// so the thread block copies its segments in 16-byte pieces
-struct CarpBlockDesc {
-  int64_t fp;     // first footprint entry (int32 global X rows), multiple of 4
-  int64_t ent;    // first matrix entry (values, uint16 footprint slots), multiple of 8
-  int64_t row;    // first row slot (uint16 entry offsets: nrows+1; (norm, diagonal) pairs), multiple of 8
-  int64_t step;   // first step start (uint16 local rows: nsteps+1), multiple of 8
-  int32_t nrows, nfp, nnz, nsteps;
-};
-
-PB_HD inline int carp_r8(int x) { return (x + 7) & ~7; }
+// One row block of the block-coloured sweep is one byte segment that the
+// thread block copies to shared memory; segment b starts at b * stride
+// (stride: the largest segment, a multiple of 16), so its address needs no
+// lookup:
+//   header     int32 nrows, nfp, nnz, nsteps
+//   fp         int32 [nfp]       global X rows of the footprint, the block's
+//                                own rows first (slots 0..nrows-1)
+//   val        T [nnz]           entries, rows in block order
+//   nd         T [2 nrows]       per row (sum_k a_ik^2, a_ii)
+//   lcol       uint16 [nnz]      footprint slot of each entry's column
+//   lrp        uint16 [nrows+1]  entry offsets of the rows
+//   step       uint16 [nsteps+1] first row of each step
+// each part starting on a 16-byte boundary.  Header and footprint rows come
+// first: the X gather needs only them (carp_seg_head bytes).
 PB_HD inline int carp_r16b(int x) { return (x + 15) & ~15; }
 
-// shared-memory layout of the block sweep kernel (byte offsets), sized for
-// the largest block; TPR slots of tsize bytes per X row
-struct CarpSmem {
-  int xs, xis, bs, val, nd, fp, lcol, lrp, step, total;
+struct CarpSeg {
+  int nrows, nfp, nnz, nsteps;
+  int fp, val, nd, lcol, lrp, step, bytes;  // byte offsets inside the segment, size
 };
-PB_HD inline CarpSmem carp_smem_layout(int max_fp, int max_rows, int max_nnz, int tpr, int tsize, bool rc,
+PB_HD inline CarpSeg carp_seg(int nrows, int nfp, int nnz, int nsteps, int tsize)
+{
+  CarpSeg g;
+  g.nrows = nrows;
+  g.nfp = nfp;
+  g.nnz = nnz;
+  g.nsteps = nsteps;
+  int o = 16;
+  g.fp = o;
+  o += carp_r16b(4 * nfp);
+  g.val = o;
+  o += carp_r16b(tsize * nnz);
+  g.nd = o;
+  o += carp_r16b(2 * tsize * nrows);
+  g.lcol = o;
+  o += carp_r16b(2 * nnz);
+  g.lrp = o;
+  o += carp_r16b(2 * (nrows + 1));
+  g.step = o;
+  o += carp_r16b(2 * (nsteps + 1));
+  g.bytes = o;
+  return g;
+}
+// bytes of header and footprint rows for footprints of at most max_fp rows
+PB_HD inline int carp_seg_head(int max_fp) { return 16 + carp_r16b(4 * max_fp); }
+
+// Shared-memory layout of the block sweep kernel (byte offsets): the X
+// footprint rows (TPR slots of tsize bytes per row; a second set for the
+// imaginary part), the block's rows of B and its segment (seg_stride bytes).
+struct CarpSmem {
+  int xs, xis, bs;
+  int xbase, mbase, total;
+};
+PB_HD inline CarpSmem carp_smem_layout(int max_fp, int max_rows, int seg_stride, int tpr, int tsize, bool rc,
                                        bool hasb)
 {
   CarpSmem L;
@@ -64,19 +99,9 @@ PB_HD inline CarpSmem carp_smem_layout(int max_fp, int max_rows, int max_nnz, in
   if (rc) o += carp_r16b(max_fp * tpr * tsize);
   L.bs = o;
   if (hasb) o += carp_r16b(max_rows * tpr * tsize);
-  L.val = o;
-  o += carp_r16b(carp_r8(max_nnz) * tsize);
-  L.nd = o;
-  o += carp_r16b(2 * carp_r8(max_rows + 1) * tsize);
-  L.fp = o;
-  o += carp_r16b(4 * ((max_fp + 3) & ~3));
-  L.lcol = o;
-  o += carp_r16b(2 * carp_r8(max_nnz));
-  L.lrp = o;
-  o += carp_r16b(2 * carp_r8(max_rows + 1));
-  L.step = o;
-  o += 2 * carp_r8(64 + 1);
-  L.total = o;
+  L.xbase = 0;
+  L.mbase = o;
+  L.total = o + carp_r16b(seg_stride);
   return L;
 }
 
@@ -210,24 +235,60 @@ inline bool carp_block_color(int64_t n, const std::vector<int64_t>& prp, const s
     for (int64_t b = 0; b < nb; b++)
       for (int64_t k = B.fp_ptr[b]; k < B.fp_ptr[b + 1]; k++) cblk[fill[B.fp[k]]++] = (int32_t)b;
   }
-  std::vector<int32_t> color(nb, -1);
-  std::vector<int64_t> mark;
-  int ncolor = 0;
-  for (int64_t b = 0; b < nb; b++) {
-    for (int64_t k = B.fp_ptr[b]; k < B.fp_ptr[b + 1]; k++) {
-      const int32_t c = B.fp[k];
-      for (int64_t t = cp[c]; t < cp[c + 1]; t++) {
-        const int32_t o = cblk[t];
-        if (o != b && color[o] >= 0) {
-          if ((int)mark.size() <= color[o]) mark.resize(color[o] + 1, -1);
-          mark[color[o]] = b;
+  // conflict lists: blocks whose footprints meet
+  std::vector<int64_t> ap(nb + 1, 0);
+  std::vector<int32_t> adj;
+  {
+    std::vector<int64_t> seen(nb, -1);
+    for (int64_t b = 0; b < nb; b++) {
+      for (int64_t k = B.fp_ptr[b]; k < B.fp_ptr[b + 1]; k++) {
+        const int32_t c = B.fp[k];
+        for (int64_t t = cp[c]; t < cp[c + 1]; t++) {
+          const int32_t o = cblk[t];
+          if (o != b && seen[o] != b) {
+            seen[o] = b;
+            adj.push_back(o);
+          }
         }
       }
+      ap[b + 1] = (int64_t)adj.size();
     }
-    int c = 0;
-    while (c < (int)mark.size() && mark[c] == b) c++;
-    color[b] = c;
-    ncolor = std::max(ncolor, c + 1);
+  }
+  // greedy colouring in a given block order, then iterated greedy (blocks
+  // visited colour class by colour class, classes in reverse order): never
+  // more colours, often fewer, i.e. fewer launches per sweep
+  std::vector<int64_t> mark;
+  auto greedy = [&](const std::vector<int32_t>& ord, std::vector<int32_t>& col) {
+    col.assign(nb, -1);
+    mark.assign(mark.size(), -1);
+    int nc = 0;
+    for (int64_t k = 0; k < nb; k++) {
+      const int64_t b = ord.empty() ? k : ord[k];
+      for (int64_t t = ap[b]; t < ap[b + 1]; t++) {
+        const int32_t co = col[adj[t]];
+        if (co >= 0) {
+          if ((int)mark.size() <= co) mark.resize(co + 1, -1);
+          mark[co] = b;
+        }
+      }
+      int c = 0;
+      while (c < (int)mark.size() && mark[c] == b) c++;
+      col[b] = c;
+      nc = std::max(nc, c + 1);
+    }
+    return nc;
+  };
+  std::vector<int32_t> color, cand, vis(nb);
+  int ncolor = greedy(std::vector<int32_t>(), color);
+  for (int round = 0; round < 8 && ncolor > 1; round++) {
+    std::vector<int64_t> start(ncolor + 1, 0);
+    for (int64_t b = 0; b < nb; b++) start[ncolor - color[b]]++;
+    for (int c = 0; c < ncolor; c++) start[c + 1] += start[c];
+    for (int64_t b = 0; b < nb; b++) vis[start[ncolor - 1 - color[b]]++] = (int32_t)b;
+    const int nc = greedy(vis, cand);
+    if (nc > ncolor) break;
+    color.swap(cand);
+    ncolor = nc;
   }
   // blocks in colour order (stable)
   std::vector<int64_t> order(nb);
@@ -312,18 +373,13 @@ inline bool carp_block_color(int64_t n, const std::vector<int64_t>& prp, const s
   return true;
 }
 
-// Device arrays of the block-coloured sweep, built from the blocks and the
-// CRS matrix (rp, col, val; n square): per block its footprint rows, its
-// entries with footprint-local columns (rows in block order, the block's own
-// rows being footprint slots 0..nrows-1), per row the entry offsets and the
-// pair (sum_k a_ik^2, a_ii), and the step starts.
+// Device array of the block-coloured sweep, built from the blocks and the
+// CRS matrix (rp, col, val; n square): the segments (layout above) at a
+// fixed stride.
 template <class T>
 struct CarpBlockLayout {
-  std::vector<CarpBlockDesc> desc;
-  std::vector<int32_t> fp;
-  std::vector<T> val, nd;
-  std::vector<uint16_t> lcol, lrp, step;
-  int max_nnz = 0;
+  std::vector<unsigned char> seg;
+  int stride = 0;
 };
 
 template <class T>
@@ -331,49 +387,53 @@ void carp_block_layout(const CarpBlocks& B, int64_t n, const int64_t* rp, const 
                        CarpBlockLayout<T>& L)
 {
   const int64_t nb = B.nblocks;
-  L.desc.assign(nb, CarpBlockDesc());
+  std::vector<CarpSeg> gs(nb);
+  L.stride = 16;
+  for (int64_t b = 0; b < nb; b++) {
+    const int64_t r0 = B.row_ptr[b], r1 = B.row_ptr[b + 1];
+    int nz = 0;
+    for (int64_t q = r0; q < r1; q++) nz += (int)(rp[B.rows[q] + 1] - rp[B.rows[q]]);
+    gs[b] = carp_seg((int)(r1 - r0), (int)(B.fp_ptr[b + 1] - B.fp_ptr[b]), nz,
+                     (int)(B.step_ptr[b + 1] - B.step_ptr[b] - 1), (int)sizeof(T));
+    L.stride = std::max(L.stride, gs[b].bytes);
+  }
+  L.seg.assign((size_t)nb * L.stride, 0);
   std::vector<int32_t> slot(n, -1);
   for (int64_t b = 0; b < nb; b++) {
     const int64_t r0 = B.row_ptr[b], r1 = B.row_ptr[b + 1];
     const int64_t f0 = B.fp_ptr[b], f1 = B.fp_ptr[b + 1];
     const int64_t s0 = B.step_ptr[b], s1 = B.step_ptr[b + 1];
-    CarpBlockDesc& d = L.desc[b];
-    d.nrows = (int32_t)(r1 - r0);
-    d.nfp = (int32_t)(f1 - f0);
-    d.nsteps = (int32_t)(s1 - s0 - 1);
-    d.fp = (int64_t)L.fp.size();
+    const CarpSeg& g = gs[b];
+    unsigned char* p = L.seg.data() + (size_t)b * L.stride;
+    const int32_t hdr[4] = {g.nrows, g.nfp, g.nnz, g.nsteps};
+    memcpy(p, hdr, sizeof(hdr));
+    int32_t* fp = (int32_t*)(p + g.fp);
+    T* v = (T*)(p + g.val);
+    T* nd = (T*)(p + g.nd);
+    uint16_t* lc = (uint16_t*)(p + g.lcol);
+    uint16_t* lr = (uint16_t*)(p + g.lrp);
+    uint16_t* st = (uint16_t*)(p + g.step);
     for (int64_t k = f0; k < f1; k++) {
       slot[B.fp[k]] = (int32_t)(k - f0);
-      L.fp.push_back(B.fp[k]);
+      fp[k - f0] = B.fp[k];
     }
-    while (L.fp.size() % 4) L.fp.push_back(0);
-    d.ent = (int64_t)L.val.size();
-    d.row = (int64_t)L.lrp.size();
-    L.lrp.push_back(0);
+    int e = 0;
+    lr[0] = 0;
     for (int64_t q = r0; q < r1; q++) {
       const int64_t i = B.rows[q];
       T sq = T(0), dg = T(0);
-      for (int64_t p = rp[i]; p < rp[i + 1]; p++) {
-        L.val.push_back(val[p]);
-        L.lcol.push_back((uint16_t)slot[col[p]]);
-        sq += val[p] * val[p];
-        if (col[p] == i) dg = val[p];
+      for (int64_t k = rp[i]; k < rp[i + 1]; k++) {
+        v[e] = val[k];
+        lc[e] = (uint16_t)slot[col[k]];
+        e++;
+        sq += val[k] * val[k];
+        if (col[k] == i) dg = val[k];
       }
-      L.lrp.push_back((uint16_t)(L.val.size() - d.ent));
-      L.nd.push_back(sq);
-      L.nd.push_back(dg);
+      lr[q - r0 + 1] = (uint16_t)e;
+      nd[2 * (q - r0)] = sq;
+      nd[2 * (q - r0) + 1] = dg;
     }
-    d.nnz = (int32_t)(L.val.size() - d.ent);
-    L.max_nnz = std::max(L.max_nnz, (int)d.nnz);
-    while (L.val.size() % 8) {
-      L.val.push_back(T(0));
-      L.lcol.push_back(0);
-    }
-    while (L.lrp.size() % 8) L.lrp.push_back(0);
-    L.nd.resize(2 * L.lrp.size(), T(0));
-    d.step = (int64_t)L.step.size();
-    for (int64_t k = s0; k < s1; k++) L.step.push_back(B.step[k]);
-    while (L.step.size() % 8) L.step.push_back(0);
+    for (int64_t k = s0; k < s1; k++) st[k - s0] = B.step[k];
     for (int64_t k = f0; k < f1; k++) slot[B.fp[k]] = -1;
   }
 }

@@ -205,6 +205,11 @@ class Runtime {
   // shared memory (pb_carp_blocks.hpp); false: one launch per class of a
   // distance-2 row colouring.  Read when the CARP work is set up.
   bool carp_blocks = true;
+  // row limit of a block (footprint limit twice that, pattern limit 16x)
+  int carp_block_rows = 128;
+  // block sweep launches with a programmatic dependency on the previous
+  // launch (overlap of its segment copies with that launch's tail)
+  bool carp_pdl = true;
 
   // statistics: kernel launches issued by this library (all lanes)
   std::atomic<uint64_t> launches{0};

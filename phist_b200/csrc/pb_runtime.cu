@@ -46,6 +46,8 @@ void Runtime::init()
   if (const char* s = getenv("PHIST_B200_SELL_SIGMA")) sell_sigma_default = atoll(s);
   if (const char* v = getenv("PHIST_B200_SPMV_PREFETCH")) spmv_pf = atoi(v) != 0;
   if (const char* v = getenv("PHIST_B200_CARP_BLOCKS")) carp_blocks = atoi(v) != 0;
+  if (const char* v = getenv("PHIST_B200_CARP_BLOCK_ROWS")) carp_block_rows = std::max(1, std::min(256, atoi(v)));
+  if (const char* v = getenv("PHIST_B200_CARP_PDL")) carp_pdl = atoi(v) != 0;
   noalloc_setup_current_device();
   inited_ = true;
 }

@@ -2,22 +2,23 @@
 // phist_b200/csrc/pb_carp.cuh) for the CPU tests: builds the blocks and the
 // device layout with the library's own host code (pb_carp_blocks.hpp), then
 // runs the kernel's schedule -- colour launches, one thread block per row
-// block, its 16-byte segment copies, footprint gather, steps and write-back
-// -- on the host with every index checked against the arrays and
-// shared-memory regions it addresses:
-//   * every segment copy stays inside its array and its shared region;
+// block: the segment head, then the rest of the segment with the X and B
+// rows, the steps and the write-back -- on the host with every index
+// checked against the arrays and shared-memory regions it addresses:
+//   * every copy stays inside its source array and its shared region;
 //   * footprint rows are valid rows of X, and blocks of one launch have
 //     disjoint footprints;
 //   * step bounds, entry offsets and footprint-local columns stay inside the
 //     block, and the rows of one step touch disjoint footprint slots.
 // Any violation exits with status 3 and a message.
 //
-// usage: carp_blocks_emu <in> <out> <max_rows> <max_fp> <max_nnz>
+// usage: carp_blocks_emu <in> <out> <max_rows> <max_fp> <max_nnz> <wide>
+//   wide 1: X and B copied in 16-byte pieces (when the column count is even)
 //   in : int64 n, nnz, nv, has_b; int64 rp[n+1]; int32 col[nnz];
 //        f64 val[nnz], shifts[nv], omega[nv], b[n*nv] (if has_b), x[n*nv]
 //   out: int64 ok (0: no block layout), nseg; int32 rows[n];
 //        int64 seg_ptr[nseg+1]; f64 x[n*nv];
-//        int64 nblocks, ncolors, max_fp, max_rows, max_nnz, max_steps,
+//        int64 nblocks, ncolors, max_fp, max_rows, seg_stride, max_steps,
 //        smem_bytes, footprint_total
 #include "../phist_b200/csrc/pb_carp_blocks.hpp"
 
@@ -52,8 +53,8 @@ static void wr(FILE* f, const V* p, size_t n)
 
 int main(int argc, char** argv)
 {
-  if (argc != 6) {
-    fprintf(stderr, "usage: %s in out max_rows max_fp max_nnz\n", argv[0]);
+  if (argc != 7) {
+    fprintf(stderr, "usage: %s in out max_rows max_fp max_nnz wide\n", argv[0]);
     return 2;
   }
   FILE* fi = fopen(argv[1], "rb");
@@ -103,112 +104,119 @@ int main(int argc, char** argv)
   carp_block_layout<double>(B, n, rp.data(), col.data(), val.data(), L);
   EMU_CHECK(B.max_steps <= 64);
   const int TPR = nv <= 1 ? 1 : nv <= 2 ? 2 : nv <= 4 ? 4 : nv <= 8 ? 8 : nv <= 16 ? 16 : 32;
-  const CarpSmem S = carp_smem_layout(B.max_fp, B.max_rows, L.max_nnz, TPR, 8, false, hasb);
+  // X and B pieces: 2 doubles (16 bytes) when the columns fill whole pieces
+  const int W = (atoi(argv[6]) != 0 && nv % 2 == 0) ? 2 : 1;
+  const int PW = TPR / W;
+  const CarpSmem S = carp_smem_layout(B.max_fp, B.max_rows, L.stride, TPR, 8, false, hasb);
+  const int head = carp_seg_head(B.max_fp);
+  EMU_CHECK(S.mbase % 16 == 0 && S.bs % 16 == 0 && L.stride % 16 == 0);
+  EMU_CHECK(head <= L.stride && (int64_t)L.seg.size() == B.nblocks * (int64_t)L.stride);
   std::vector<unsigned char> smem(S.total);
   std::vector<int64_t> owner(n, -1);
   int64_t launch_id = 0;
 
+  // the thread block of row block blk
   auto run_block = [&](int64_t blk, int dir) {
-    const CarpBlockDesc d = L.desc[blk];
-    EMU_CHECK(d.nfp <= B.max_fp && d.nrows <= B.max_rows && d.nnz <= L.max_nnz && d.nrows <= d.nfp);
     memset(smem.data(), 0xff, smem.size());
-    auto seg = [&](const void* base, size_t bytes, int64_t off, int nchunks, int s0, int s1) {
-      EMU_CHECK(off % 16 == 0);
-      EMU_CHECK(off + 16 * (int64_t)nchunks <= (int64_t)bytes);
-      EMU_CHECK(s0 + 16 * nchunks <= s1);
-      memcpy(smem.data() + s0, (const char*)base + off, 16 * (size_t)nchunks);
-    };
-    seg(L.val.data(), L.val.size() * 8, d.ent * 8, carp_r8(d.nnz) * 8 / 16, S.val, S.nd);
-    seg(L.lcol.data(), L.lcol.size() * 2, d.ent * 2, carp_r8(d.nnz) * 2 / 16, S.lcol, S.lrp);
-    seg(L.lrp.data(), L.lrp.size() * 2, d.row * 2, carp_r8(d.nrows + 1) * 2 / 16, S.lrp, S.step);
-    seg(L.nd.data(), L.nd.size() * 8, d.row * 16, carp_r8(d.nrows) * 2 * 8 / 16, S.nd, S.fp);
-    seg(L.fp.data(), L.fp.size() * 4, d.fp * 4, ((d.nfp + 3) & ~3) * 4 / 16, S.fp, S.lcol);
-    seg(L.step.data(), L.step.size() * 2, d.step * 2, carp_r8(d.nsteps + 1) * 2 / 16, S.step, S.total);
-    double* xs = (double*)(smem.data() + S.xs);
-    double* bs = (double*)(smem.data() + S.bs);
-    const double* vs = (const double*)(smem.data() + S.val);
-    const double* nds = (const double*)(smem.data() + S.nd);
-    const int32_t* fps = (const int32_t*)(smem.data() + S.fp);
-    const uint16_t* lcs = (const uint16_t*)(smem.data() + S.lcol);
-    const uint16_t* lrs = (const uint16_t*)(smem.data() + S.lrp);
-    const uint16_t* sts = (const uint16_t*)(smem.data() + S.step);
-    for (int e = 0; e < d.nfp * TPR; e++) {
-      const int u = e / TPR, j = e % TPR;
+    unsigned char* mb = smem.data() + S.mbase;
+    unsigned char* xb = smem.data() + S.xbase;
+    const int64_t off = blk * (int64_t)L.stride;
+    // H: header and footprint rows
+    EMU_CHECK(off + head <= (int64_t)L.seg.size());
+    EMU_CHECK(S.mbase + head <= S.total);
+    memcpy(mb, L.seg.data() + off, head);
+    // X: rest of the segment, X and B rows
+    const int32_t* hdr = (const int32_t*)mb;
+    const CarpSeg sg = carp_seg(hdr[0], hdr[1], hdr[2], hdr[3], 8);
+    EMU_CHECK(sg.bytes % 16 == 0 && sg.bytes <= L.stride && S.mbase + sg.bytes <= S.total);
+    if (sg.bytes > head) memcpy(mb + head, L.seg.data() + off + head, sg.bytes - head);
+    EMU_CHECK(sg.nfp <= B.max_fp && sg.nrows <= B.max_rows && sg.nrows <= sg.nfp);
+    const int32_t* fps = (const int32_t*)(mb + 16);
+    double* xs = (double*)(xb + S.xs);
+    double* bs = (double*)(xb + S.bs);
+    for (int e = 0; e < sg.nfp * PW; e++) {
+      const int u = e / PW, j = (e % PW) * W;
       if (j >= nv) continue;
-      EMU_CHECK(d.fp + u < (int64_t)L.fp.size());
-      const int64_t g = L.fp[d.fp + u];
+      EMU_CHECK(16 + 4 * (u + 1) <= head);
+      const int64_t g = fps[u];
       EMU_CHECK(g >= 0 && g < n);
-      EMU_CHECK(S.xs + 8 * (e + 1) <= S.xis);
+      EMU_CHECK(S.xs + 8 * (u * TPR + j + W) <= S.xis);
       if (j == 0) {
         EMU_CHECK(owner[g] != launch_id);  // disjoint footprints in one launch
         owner[g] = launch_id;
       }
-      xs[e] = x[g * nv + j];
+      for (int k = 0; k < W; k++) xs[u * TPR + j + k] = x[g * nv + j + k];
     }
     if (hasb)
-      for (int e = 0; e < d.nrows * TPR; e++) {
-        const int r = e / TPR, j = e % TPR;
+      for (int e = 0; e < sg.nrows * PW; e++) {
+        const int r = e / PW, j = (e % PW) * W;
         if (j >= nv) continue;
-        EMU_CHECK(S.bs + 8 * (e + 1) <= S.val);
-        bs[e] = b[(int64_t)L.fp[d.fp + r] * nv + j];
+        EMU_CHECK(S.bs + 8 * (r * TPR + j + W) <= S.mbase);
+        for (int k = 0; k < W; k++) bs[r * TPR + j + k] = b[(int64_t)fps[r] * nv + j + k];
       }
-    EMU_CHECK(d.nsteps >= 1 && d.nsteps <= 64 && sts[0] == 0 && sts[d.nsteps] == d.nrows);
-    std::vector<int> touched(d.nfp);
-    auto step = [&](int s) {
-      const int lo = sts[s], hi = sts[s + 1];
-      EMU_CHECK(lo <= hi && hi <= d.nrows);
+    const double* vs = (const double*)(mb + sg.val);
+    const double* nds = (const double*)(mb + sg.nd);
+    const uint16_t* lcs = (const uint16_t*)(mb + sg.lcol);
+    const uint16_t* lrs = (const uint16_t*)(mb + sg.lrp);
+    const uint16_t* sts = (const uint16_t*)(mb + sg.step);
+    EMU_CHECK(sg.nsteps >= 1 && sg.nsteps <= 64 && sts[0] == 0 && sts[sg.nsteps] == sg.nrows);
+    std::vector<int> touched(sg.nfp);
+    auto step = [&](int st) {
+      const int lo = sts[st], hi = sts[st + 1];
+      EMU_CHECK(lo <= hi && hi <= sg.nrows);
       std::fill(touched.begin(), touched.end(), -1);
       for (int r = lo; r < hi; r++) {
-        EMU_CHECK(lrs[r] <= lrs[r + 1] && lrs[r + 1] <= d.nnz);
+        EMU_CHECK(lrs[r] <= lrs[r + 1] && lrs[r + 1] <= sg.nnz);
         auto touch = [&](int sl) {
-          EMU_CHECK(sl >= 0 && sl < d.nfp);
+          EMU_CHECK(sl >= 0 && sl < sg.nfp);
           EMU_CHECK(touched[sl] == -1 || touched[sl] == r);
           touched[sl] = r;
         };
         touch(r);
         for (int p = lrs[r]; p < lrs[r + 1]; p++) touch(lcs[p]);
       }
-      for (int e = 0; e < (hi - lo) * TPR; e++) {
-        const int r = lo + e / TPR, j = e % TPR;
-        if (j >= nv) continue;
-        const double s_ = sr[j];
-        double tr = -s_ * xs[r * TPR + j];
-        for (int p = lrs[r]; p < lrs[r + 1]; p++) tr += vs[p] * xs[lcs[p] * TPR + j];
-        if (hasb) tr -= bs[r * TPR + j];
-        double rn = nds[2 * r] - 2.0 * nds[2 * r + 1] * s_ + s_ * s_;
-        if (rn == 0.0) rn = 1.0;
-        tr *= om[j] / rn;
-        xs[r * TPR + j] += tr * s_;
-        for (int p = lrs[r]; p < lrs[r + 1]; p++) xs[lcs[p] * TPR + j] -= tr * vs[p];
-      }
+      for (int r = lo; r < hi; r++)
+        for (int j = 0; j < nv; j++) {
+          const double s_ = sr[j];
+          double rn = nds[2 * r] - 2.0 * nds[2 * r + 1] * s_ + s_ * s_;
+          if (rn == 0.0) rn = 1.0;
+          const double f = om[j] / rn;
+          double tr = -s_ * xs[r * TPR + j];
+          for (int p = lrs[r]; p < lrs[r + 1]; p++) tr += vs[p] * xs[lcs[p] * TPR + j];
+          if (hasb) tr -= bs[r * TPR + j];
+          tr *= f;
+          xs[r * TPR + j] += tr * s_;
+          for (int p = lrs[r]; p < lrs[r + 1]; p++) xs[lcs[p] * TPR + j] -= tr * vs[p];
+        }
     };
     if (dir & 1)
-      for (int s = 0; s < d.nsteps; s++) step(s);
+      for (int st = 0; st < sg.nsteps; st++) step(st);
     if (dir & 2)
-      for (int s = d.nsteps - 1; s >= 0; s--) step(s);
-    for (int e = 0; e < d.nfp * TPR; e++) {
-      const int u = e / TPR, j = e % TPR;
+      for (int st = sg.nsteps - 1; st >= 0; st--) step(st);
+    for (int e = 0; e < sg.nfp * PW; e++) {
+      const int u = e / PW, j = (e % PW) * W;
       if (j >= nv) continue;
       const int64_t g = fps[u];
-      EMU_CHECK(g == L.fp[d.fp + u]);
-      x[g * nv + j] = xs[e];
+      for (int k = 0; k < W; k++) x[g * nv + j + k] = xs[u * TPR + j + k];
     }
   };
   auto launch = [&](int c, int dir) {
     for (int64_t blk = B.color_ptr[c]; blk < B.color_ptr[c + 1]; blk++) run_block(blk, dir);
     launch_id++;
   };
+  // forward over the colours, the last one forward and straight back, then
+  // backward over the others
   const int C = B.ncolors;
   for (int c = 0; c < C - 1; c++) launch(c, 1);
   launch(C - 1, 3);
   for (int c = C - 2; c >= 0; c--) launch(c, 2);
 
-  const int64_t head[2] = {1, (int64_t)B.seq_ptr.size() - 1};
-  wr(fo, head, 2);
+  const int64_t ohead[2] = {1, (int64_t)B.seq_ptr.size() - 1};
+  wr(fo, ohead, 2);
   wr(fo, B.seq_rows.data(), B.seq_rows.size());
   wr(fo, B.seq_ptr.data(), B.seq_ptr.size());
   wr(fo, x.data(), x.size());
-  const int64_t st[8] = {B.nblocks, B.ncolors, B.max_fp, B.max_rows, L.max_nnz, B.max_steps, S.total,
+  const int64_t st[8] = {B.nblocks, B.ncolors, B.max_fp, B.max_rows, L.stride, B.max_steps, S.total,
                          (int64_t)B.fp.size()};
   wr(fo, st, 8);
   fclose(fo);

@@ -3,10 +3,11 @@ on the CPU.
 
 tests/carp_blocks_emu.cpp builds the row blocks, their colouring, steps and
 device arrays with the library's own host code (phist_b200/csrc/
-pb_carp_blocks.hpp) and runs the sweep kernel's schedule on the host with
-every copy and index checked against the array or shared-memory region it
-addresses (blocks of one launch have disjoint footprints, rows of one step
-touch disjoint slots).  The result must equal the oracle's sequential
+pb_carp_blocks.hpp) and runs the sweep kernel's schedule (X copied in
+16-byte pieces or element by element) on the host with every copy and
+index checked against the array or shared-memory region it addresses
+(blocks of one launch with disjoint footprints, rows of one step touching
+disjoint slots).  The result must equal the oracle's sequential
 Kaczmarz sweep (kacz_sub_def.h formulae) over the reported row order to
 1e-13 (the oracle forms row norms and sums in its own order), and every
 segment of that order must be a distance-2 independent set -- the facts the
@@ -31,7 +32,7 @@ def emu(tmp_path_factory):
     subprocess.run(["g++", "-O2", "-std=c++17", "-Wall", "-Werror", "-o", exe, SRC], check=True)
     k = [0]
 
-    def run(rp, col, val, shifts, omega, b, x0, max_rows=128, max_fp=256, max_nnz=2048):
+    def run(rp, col, val, shifts, omega, b, x0, max_rows=128, max_fp=256, max_nnz=2048, wide=1):
         k[0] += 1
         fin, fout = str(d / f"in{k[0]}"), str(d / f"out{k[0]}")
         n, nv = x0.shape
@@ -45,7 +46,8 @@ def emu(tmp_path_factory):
             if b is not None:
                 np.ascontiguousarray(b, np.float64).tofile(f)
             np.ascontiguousarray(x0, np.float64).tofile(f)
-        r = subprocess.run([exe, fin, fout, str(max_rows), str(max_fp), str(max_nnz)], capture_output=True, text=True)
+        r = subprocess.run([exe, fin, fout, str(max_rows), str(max_fp), str(max_nnz), str(wide)],
+                           capture_output=True, text=True)
         assert r.returncode == 0, r.stderr
         raw = open(fout, "rb").read()
         ok, nseg = np.frombuffer(raw[:16], np.int64)
@@ -59,7 +61,7 @@ def emu(tmp_path_factory):
         x = np.frombuffer(raw[o:o + 8 * n * nv], np.float64).reshape(n, nv)
         o += 8 * n * nv
         st = np.frombuffer(raw[o:o + 64], np.int64)
-        stats = dict(zip(["nblocks", "ncolors", "max_fp", "max_rows", "max_nnz", "max_steps", "smem", "fp_total"],
+        stats = dict(zip(["nblocks", "ncolors", "max_fp", "max_rows", "seg_stride", "max_steps", "smem", "fp_total"],
                          st.tolist()))
         return rows, seg, x, stats
     return run
@@ -100,9 +102,10 @@ def _check(emu, oracle, rp, c, v, nvec, with_b=True, seed=0, **kw):
 @pytest.mark.parametrize("prob", ["sprandn388", "sprandn_nodiag388", "symmMat20", "spshift388", "jadaTestMat512",
                                   "spshift25", "speye25", "sprandsym163"])
 @pytest.mark.parametrize("nvec", [1, 3, 8])
-def test_phist_testmats(emu, oracle, testmats, prob, nvec):
+@pytest.mark.parametrize("wide", [1, 0])
+def test_phist_testmats(emu, oracle, testmats, prob, nvec, wide):
     rp, c, v, shape = testmats(prob)
-    _check(emu, oracle, rp, c, v, nvec, seed=nvec)
+    _check(emu, oracle, rp, c, v, nvec, seed=nvec, wide=wide)
 
 
 @pytest.mark.parametrize("nvec", [1, 8, 16, 32])
@@ -127,6 +130,7 @@ def test_rhs_null_and_small_blocks(emu, oracle):
     from phist_b200 import generators as G
     rp, c, v = G.honeycomb(12, 10, 1)
     _check(emu, oracle, rp, c, v, 2, with_b=False)
+    _check(emu, oracle, rp, c, v, 2, with_b=False, wide=0)
     _check(emu, oracle, rp, c, v, 2, max_rows=1, max_fp=4, max_nnz=4)
     _check(emu, oracle, rp, c, v, 5, max_rows=7, max_fp=12, max_nnz=40)
 

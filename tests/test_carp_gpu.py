@@ -16,7 +16,7 @@ import ctypes as ct
 import numpy as np
 import pytest
 
-from conftest import relerr
+from conftest import relerr, sort_rows
 
 pytestmark = pytest.mark.gpu
 
@@ -221,6 +221,52 @@ def test_carp_sweep_strided_views(session, layout, oracle):
     assert relerr(full[:, 2:5], ref) < 1e-13
     K.chk(K.phist_Dcarp_destroy, A.h, work)
     for o in (X, B, Xw, Bw, A):
+        o.delete()
+
+
+def test_carp_sweep_repeated_columns(session, layout, oracle):
+    """rows that hold a column twice (the diagonal split into two entries and
+    an off-diagonal entry repeated): every entry is its own projection term,
+    as in the sequential sweep"""
+    from phist_b200 import generators as G
+    from phist_b200 import kernels as K
+    from phist_b200.objects import Mvec, SparseMat
+    rp0, c0, v0 = G.honeycomb(20, 16, 5)
+    n = len(rp0) - 1
+    rows_c, rows_v = [], []
+    for i in range(n):
+        cc = list(c0[rp0[i]:rp0[i + 1]])
+        vv = list(v0[rp0[i]:rp0[i + 1]])
+        if i % 3 == 0:
+            k = cc.index(i)
+            vv[k] *= 0.5
+            cc.append(i)
+            vv.append(vv[k])
+        if i % 5 == 1:
+            cc.append(cc[0])
+            vv.append(0.25)
+        rows_c.append(cc)
+        rows_v.append(vv)
+    rp = np.zeros(n + 1, np.int64)
+    rp[1:] = np.cumsum([len(x) for x in rows_c])
+    # the library keeps the entries of a row stably sorted by column
+    rp, c, v = sort_rows(rp, np.concatenate(rows_c).astype(np.int32), np.concatenate(rows_v))
+    A = SparseMat.from_crs(rp, c, v)
+    nvec = 4
+    rng = np.random.default_rng(17)
+    shifts = rng.uniform(-1, 1, nvec)
+    omega = rng.uniform(0.8, 1.4, nvec)
+    x0 = rng.uniform(-1, 1, (n, nvec))
+    b = rng.uniform(-1, 1, (n, nvec))
+    work, sh = _setup(A, shifts)
+    rows, _ = _order(work, n)
+    X = Mvec(A.row_map, nvec).set(x0)
+    B = Mvec(A.row_map, nvec).set(b)
+    K.chk(K.phist_Dcarp_sweep, A.h, K.sptr(sh, np.float64), B.h, X.h, work, K.sptr(omega, np.float64))
+    ref = oracle.carp_sweep(rp, c, v, shifts, b, x0, omega, order=rows)
+    assert relerr(X.get(), ref) < 1e-13
+    K.chk(K.phist_Dcarp_destroy, A.h, work)
+    for o in (X, B, A):
         o.delete()
 
 
