@@ -11,10 +11,12 @@ with the block-vector term multiplied by nvec).
 
     python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference]
 
---impl reference times the CPU restatement of PHIST's builtin SpMMV
-(oracle/, the same loop order as spmvm_kernels.F90; PHIST's own kernels are
-Fortran+MPI and are not buildable here) on all host cores, on a bounded
-sample of the same workload.  Under torchrun only rank 0 runs that arm.
+--impl reference times PHIST's builtin SpMMV on all host cores, as PHIST
+dispatches it: widths 1, 2, 4, 8 on PHIST's own C kernels (compiled from the
+PHIST sources into oracle/_ref), the other widths on the oracle's C
+restatement of the Fortran loop PHIST uses for them (its Fortran+MPI build
+is not possible here), on a bounded sample of the same workload.  Under
+torchrun only rank 0 runs that arm.
 """
 import argparse
 import json
@@ -106,7 +108,12 @@ class ClockSampler:
 
 
 def cpu_baseline(steps_budget_s=12.0, nvecs=NVECS):
-    """oracle SpMMV (CPU restatement of the builtin loop) on all host cores"""
+    """PHIST's SpMMV on all host cores, as PHIST dispatches it: widths 1, 2,
+    4, 8 on PHIST's own C kernels (dspmvm_nt_*_c, spmvm_kernels_nt.c,
+    compiled from the PHIST sources into oracle/_ref), the other widths on
+    the oracle's C restatement of the Fortran loop they take
+    (spmvm_kernels.F90:494-523); all widths on the restatement when the
+    compiled kernels are absent"""
     from oracle import oracle as O
     from phist_b200 import generators as G
     O.set_threads(os.cpu_count() or 1)
@@ -117,26 +124,41 @@ def cpu_baseline(steps_budget_s=12.0, nvecs=NVECS):
     ys = {k: np.zeros((n, k)) for k in nvecs}
     lib = O.lib()
     P = O._p
-    # warm-up
+    have_ref = O.ref_available()
+    runs = {}
     for k in nvecs:
-        lib.orc_spmmv(n, P(rp), P(c), P(v), k, 1.0, None, P(xs[k]), k, 0.0, P(ys[k]), k)
-    total_b, total_t, passes = 0.0, 0.0, 0
+        if have_ref and k in (1, 2, 4, 8):
+            runs[k] = ("phist_c", O.ref_spmmv_nt_runner(rp, c, v, xs[k])[0])
+        else:
+            def port(k=k):
+                lib.orc_spmmv(n, P(rp), P(c), P(v), k, 1.0, None, P(xs[k]), k, 0.0, P(ys[k]), k)
+            runs[k] = ("port", port)
+    for k in nvecs:  # warm-up
+        runs[k][1]()
+    tk = {k: 0.0 for k in nvecs}
+    passes = 0
     t_end = time.perf_counter() + steps_budget_s
     while passes < 1 or time.perf_counter() < t_end:
         for k in nvecs:
             t0 = time.perf_counter()
-            lib.orc_spmmv(n, P(rp), P(c), P(v), k, 1.0, None, P(xs[k]), k, 0.0, P(ys[k]), k)
-            total_t += time.perf_counter() - t0
-            total_b += spmv_bytes(n, nnz, k)
+            runs[k][1]()
+            tk[k] += time.perf_counter() - t0
         passes += 1
         if passes >= 50:
             break
+    total_t = sum(tk.values())
+    total_b = passes * sum(spmv_bytes(n, nnz, k) for k in nvecs)
+    widths = {str(k): {"impl": runs[k][0], "GBs": round(passes * spmv_bytes(n, nnz, k) / tk[k] / 1e9, 2)}
+              for k in nvecs}
+    ref_widths = [k for k in nvecs if runs[k][0] == "phist_c"]
     return {"value": round(total_b / total_t / 1e9, 3), "unit": UNIT, "cores": O.num_threads(),
-            "kind": "port",
-            "sample": "%d full passes of the nvec sweep {%s} on the same L=128 Anderson matrix (CRS, "
-                      "columns sorted), C restatement of PHIST builtin dspmvm (spmvm_kernels.F90:494-523), "
-                      "OpenMP static over rows; bit-identical to PHIST's own nvec<=8 C kernels in tests"
-                      % (passes, ",".join(map(str, nvecs))),
+            "kind": "reference" if ref_widths else "port",
+            "sample": "%d full passes of the nvec sweep {%s} on the same L=128 Anderson matrix (CRS, columns "
+                      "sorted), OpenMP static over rows; widths {%s} on PHIST's own C kernels (dspmvm_nt_*_c, "
+                      "spmvm_kernels_nt.c, compiled from source), the others on the C restatement of PHIST's "
+                      "Fortran loop (spmvm_kernels.F90:494-523), which those widths take in PHIST"
+                      % (passes, ",".join(map(str, nvecs)), ",".join(map(str, ref_widths))),
+            "widths": widths,
             "seconds": round(total_t, 3)}
 
 
@@ -162,7 +184,7 @@ def run_reference(args, rank, world):
             "data": "synthetic (seeded generator, ANDERSON3D L=128 seed 1)",
             "config": {"workload": "spmmv_anderson3d_L128_nvec_sweep", "problem": PROBLEM,
                        "n": L ** 3, "nnz": 7 * L ** 3, "nvec": NVECS, "format": "CRS (host)"},
-            "cpu_baseline": {k: cb[k] for k in ("value", "unit", "cores", "kind", "sample")},
+            "cpu_baseline": {k: cb[k] for k in ("value", "unit", "cores", "kind", "sample", "widths")},
             "e2e": {"value": cb["value"], "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
     print(json.dumps(line), flush=True)
     return 0

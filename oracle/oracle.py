@@ -290,6 +290,49 @@ def ref_spmmv_nt(rowptr, col, val, x, alpha=1.0, shifts=None, prec=False):
     return np.array(ya)
 
 
+def ref_spmmv_nt_runner(rowptr, col, val, x, alpha=1.0):
+    """PHIST's dspmvm_nt_<nvec>_c / dspmvm_nt_strided_<nvec>_c (nvec 1, 2, 4,
+    8; beta = 0) on buffers prepared once (1-based indices, 64-byte aligned
+    vectors): returns (run, y), run() computing y = alpha A x again.  For
+    timing the reference kernels without the set-up in the timed region."""
+    plain, _ = ref_libs()
+    n = len(rowptr) - 1
+    nvec = x.shape[1]
+    keep = {}
+    keep["rp1"] = np.ascontiguousarray(rowptr + 1, np.int64)
+    keep["halo"] = np.ascontiguousarray(rowptr[1:] + 1, np.int64)
+    keep["col1"] = np.ascontiguousarray(col + 1, np.int32)
+    keep["val"] = np.ascontiguousarray(val, np.float64)
+    keep["sh"] = np.zeros(nvec)
+    keep["hal"] = np.zeros(8)
+
+    def aligned(shape):
+        nb = int(np.prod(shape)) * 8
+        raw = np.zeros(nb + 64, np.uint8)
+        off = (-raw.ctypes.data) % 64
+        keep.setdefault("raw", []).append(raw)
+        return raw[off:off + nb].view(np.float64).reshape(shape)
+    xa = aligned(x.shape)
+    xa[...] = x
+    ya = aligned((n, nvec))
+    d, i32 = ct.c_double, ct.c_int
+    if nvec == 1:
+        f = plain.dspmvm_nt_1_c
+        f.argtypes = [i32, d] + [ct.c_void_p] * 8
+        args = (n, alpha, _p(keep["rp1"]), _p(keep["halo"]), _p(keep["col1"]), _p(keep["val"]), _p(keep["sh"]),
+                _p(xa), _p(keep["hal"]), _p(ya))
+    else:
+        f = getattr(plain, "dspmvm_nt_strided_%d_c" % nvec)
+        f.argtypes = [i32, d] + [ct.c_void_p] * 6 + [i32, ct.c_void_p, ct.c_void_p, i32]
+        args = (n, alpha, _p(keep["rp1"]), _p(keep["halo"]), _p(keep["col1"]), _p(keep["val"]), _p(keep["sh"]),
+                _p(xa), nvec, _p(keep["hal"]), _p(ya), nvec)
+
+    def run():
+        f(*args)
+    run.keep = (keep, xa)  # the buffers live as long as run
+    return run, ya
+
+
 def ref_ddot_prec(x, y):
     """PHIST's compensated dot (ddot_prec_<nvec>, dot_kernels_prec.c), nvec 1|2|4"""
     _, precl = ref_libs()
