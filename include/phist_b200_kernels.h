@@ -477,6 +477,12 @@ void phist_b200_SsparseMat_get_tuning(phist_Sconst_sparseMat_ptr A, int* C, int6
                                       int* unroll, int* staged, int* iflag);
 /* wait for all work this library enqueued */
 void phist_b200_synchronize(int* iflag);
+/* failure-path check of the bounded device waits: runs one kernel whose
+ * mbarrier wait cannot complete; the wait gives up after about one second,
+ * stores its code in the device error word and the kernel returns, so the
+ * call ends with PHIST_FUNCTIONAL_ERROR (-1) and a message, as a real
+ * timed-out copy would; the word is cleared and the context stays usable */
+void phist_b200_selftest_bounded_wait(int* iflag);
 /* Every host thread that calls the library works on its own lane: a CUDA
  * stream with its own scratch, counters, result mailbox and device-memory
  * cache, so solves driven from several threads overlap on the GPU.  Objects

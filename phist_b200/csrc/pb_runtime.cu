@@ -5,6 +5,7 @@
 #include <string>
 
 #include "pb_core.hpp"
+#include "pb_tma.cuh"
 
 
 namespace pb {
@@ -46,7 +47,7 @@ void Runtime::init()
   if (const char* s = getenv("PHIST_B200_SELL_SIGMA")) sell_sigma_default = atoll(s);
   if (const char* v = getenv("PHIST_B200_SPMV_PREFETCH")) spmv_pf = atoi(v) != 0;
   if (const char* v = getenv("PHIST_B200_CARP_BLOCKS")) carp_blocks = atoi(v) != 0;
-  if (const char* v = getenv("PHIST_B200_CARP_BLOCK_ROWS")) carp_block_rows = std::max(1, std::min(256, atoi(v)));
+  if (const char* v = getenv("PHIST_B200_CARP_BLOCK_ROWS")) carp_block_rows = std::max(0, std::min(256, atoi(v)));
   if (const char* v = getenv("PHIST_B200_CARP_PDL")) carp_pdl = atoi(v) != 0;
   noalloc_setup_current_device();
   inited_ = true;
@@ -563,6 +564,37 @@ void phist_b200_synchronize(int* iflag)
 {
   PB_API_BEGIN(iflag);
   if (rt().initialized()) rt().sync();
+  PB_API_END(iflag);
+}
+
+}  // extern "C"
+
+namespace pb {
+// One thread waits, bounded, on an mbarrier that nothing completes: the wait
+// runs out after about a second and stores its code in the device error
+// word, exactly as a production kernel's timed-out copy wait does.
+__global__ void k_bounded_wait_probe(int* err)
+{
+  __shared__ uint64_t bar;
+  if (threadIdx.x == 0) {
+    mbar_init(&bar, 1);
+    mbar_fence_init();
+  }
+  __syncthreads();
+  if (threadIdx.x == 0) mbar_wait(&bar, 0u, err);
+  __syncthreads();
+}
+}  // namespace pb
+
+extern "C" {
+
+void phist_b200_selftest_bounded_wait(int* iflag)
+{
+  PB_API_BEGIN(iflag);
+  pb::rt().init();
+  pb::k_bounded_wait_probe<<<1, 32, 0, pb::stream()>>>(pb::rt().device_error_word());
+  PB_LAUNCH_CHECK();
+  pb::rt().sync();  // reports the timed-out wait and clears the word
   PB_API_END(iflag);
 }
 

@@ -115,6 +115,7 @@ for _b in ("load", "store", "copy", "triad"):
     _d("phist_bench_stream_" + _b, [_ct.POINTER(_ct.c_double), _ct.POINTER(_ct.c_double), c_int_p])
 _d("phist_b200_set_sell_params", [c_int, _ct.c_int64, c_int_p])
 _d("phist_b200_synchronize", [c_int_p])
+_d("phist_b200_selftest_bounded_wait", [c_int_p])
 _d("phist_b200_lane_count", [c_int_p, c_int_p])
 _d("phist_b200_device_memory", [_ct.POINTER(u64), _ct.POINTER(u64), c_int_p])
 _d("phist_b200_set_spmv_config", [c_int, c_int, c_int, c_int_p])
