@@ -1473,17 +1473,19 @@ RowGemmArgs<T> rowgemm_args()
 // CARP
 // ======================================================================
 // Block-coloured layout (pb_carp_blocks.hpp): blocks of at most R rows
-// (runtime carp_block_rows, 128 by default) whose footprint has at most 2R
-// rows of X and whose pattern at most 16R entries.  False when the matrix has
+// whose footprint has at most 2R rows of X and whose pattern at most 16R
+// entries; R is the runtime carp_block_rows, or, when that is 0, 128 for
+// sweeps of up to 8 columns, 96 up to 16 and 64 beyond (width: the number
+// of columns the sweeps are expected to have).  False when the matrix has
 // rows too long for that, or a block needs more than 64 steps; the caller
 // then uses the row colouring.
 template <class T>
 bool carp_build_blocks(const SparseMat<T>* A, const std::vector<int64_t>& prp, const std::vector<int32_t>& pcol,
-                       CarpWork<T>* w)
+                       int width, CarpWork<T>* w)
 {
   const int64_t n = A->nrows;
   CarpBlocks B;
-  const int R = rt().carp_block_rows;
+  const int R = rt().carp_block_rows > 0 ? rt().carp_block_rows : width <= 8 ? 128 : width <= 16 ? 96 : 64;
   if (!carp_block_partition(n, prp, pcol, R, 2 * R, 16 * R, B)) return false;
   if (!carp_block_color(n, prp, pcol, B)) return false;
   CarpBlockLayout<T> L;
@@ -1515,7 +1517,7 @@ bool carp_build_blocks(const SparseMat<T>* A, const std::vector<int64_t>& prp, c
 }
 
 template <class T>
-CarpWork<T>* carp_build(const SparseMat<T>* A, int nshifts, const T* sr, const T* si)
+CarpWork<T>* carp_build(const SparseMat<T>* A, int nshifts, const T* sr, const T* si, int width = 0)
 {
   PB_REQUIRE(A->nrows == A->ncols, PB_INVALID_INPUT, "CARP needs a square matrix");
   CarpWork<T>* w = new CarpWork<T>();
@@ -1540,7 +1542,7 @@ CarpWork<T>* carp_build(const SparseMat<T>* A, int nshifts, const T* sr, const T
     prp[i + 1] = (int64_t)pcol.size();
   }
   w->nrows = n;
-  if (rt().carp_blocks && n > 0 && carp_build_blocks(A, prp, pcol, w)) {
+  if (rt().carp_blocks && n > 0 && carp_build_blocks(A, prp, pcol, width > 0 ? width : nshifts, w)) {
     rt().sync();
     return w;
   }

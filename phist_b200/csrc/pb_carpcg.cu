@@ -719,10 +719,10 @@ void phist_b200_DcarpCG_tune_block(const void* vA, int nsys, int mixed, int reps
     int e = 0;
     phist_b200_sparseMat_DtoS(vA, &s.a, &e);
     PB_REQUIRE(e == 0 && s.a, e ? e : PB_FUNCTIONAL_ERROR, "FP32 copy of the matrix failed");
-    WorkGuard<float> g{carp_build<float>(SP<float>(s.a), 1, &zs, nullptr)};
+    WorkGuard<float> g{carp_build<float>(SP<float>(s.a), 1, &zs, nullptr, std::min(nsys, 16))};
     *block = carpcg_tune_block<float>(SP<float>(s.a), g.w, nsys, reps, iter_us);
   } else {
-    WorkGuard<double> g{carp_build<double>(A, 1, &zd, nullptr)};
+    WorkGuard<double> g{carp_build<double>(A, 1, &zd, nullptr, std::min(nsys, 16))};
     *block = carpcg_tune_block<double>(A, g.w, nsys, reps, iter_us);
   }
   PB_API_END(iflag);
@@ -750,8 +750,9 @@ void phist_b200_DcarpCG_batch(const void* vA, int nsys, const double* sigma, con
   PB_REQUIRE(tol > 0.0 && maxIter > 0 && checkEvery > 0, PB_INVALID_INPUT, "tol, maxIter, checkEvery must be > 0");
   int unconverged = 0;
   if (nsys > 0) {
-    // the colouring does not depend on the slot count or the shifts: built
-    // once, used by the block tuner (block <= 0) and the solver
+    // the colouring does not depend on the shifts: built once, for the
+    // given slot count or, when the tuner picks it, for 16 slots (what it
+    // picks on the benchmark matrices), and used by the tuner and the solver
     const float zs = 0.0f;
     const double zd = 0.0;
     if (mixed) {
@@ -760,12 +761,12 @@ void phist_b200_DcarpCG_batch(const void* vA, int nsys, const double* sigma, con
       phist_b200_sparseMat_DtoS(vA, &s.a, &e);
       PB_REQUIRE(e == 0 && s.a, e ? e : PB_FUNCTIONAL_ERROR, "FP32 copy of the matrix failed");
       const SparseMat<float>* As = SP<float>(s.a);
-      WorkGuard<float> g{carp_build<float>(As, 1, &zs, nullptr)};
+      WorkGuard<float> g{carp_build<float>(As, 1, &zs, nullptr, block >= 1 ? block : std::min(nsys, 16))};
       const int w = block >= 1 ? std::min(block, nsys) : carpcg_tune_block<float>(As, g.w, nsys, 3, nullptr);
       unconverged = carpcg_batch<float>(A, As, g.w, nsys, sigma, B, X, w, tol, maxIter, checkEvery,
                                         innerTol > 0.0 ? innerTol : 1e-5, iters, relres);
     } else {
-      WorkGuard<double> g{carp_build<double>(A, 1, &zd, nullptr)};
+      WorkGuard<double> g{carp_build<double>(A, 1, &zd, nullptr, block >= 1 ? block : std::min(nsys, 16))};
       const int w = block >= 1 ? std::min(block, nsys) : carpcg_tune_block<double>(A, g.w, nsys, 3, nullptr);
       unconverged = carpcg_batch<double>(A, A, g.w, nsys, sigma, B, X, w, tol, maxIter, checkEvery, tol, iters,
                                          relres);
