@@ -215,7 +215,8 @@ __global__ void __launch_bounds__(NT) k_kacz_blocks(KaczBlockArgs<T> a)
 {
   constexpr int CPT = (TPR >= 16 / (int)sizeof(T)) ? 16 / (int)sizeof(T) : TPR;  // columns per thread
   constexpr int TPRC = TPR / CPT;                                                  // threads per row
-  constexpr int RE = 4;  // entries of a row held in registers
+  constexpr int RE = 4;  // row length of the register path
+  static_assert(NT % TPRC == 0, "a thread keeps its columns in every step");
   using V = CarpVec<T, CPT>;
   extern __shared__ __align__(16) unsigned char smem[];
   const CarpSmem L = carp_smem_layout(a.max_fp, a.max_rows, a.seg_stride, TPR, (int)sizeof(T), RC, a.b != nullptr);
@@ -282,19 +283,28 @@ __global__ void __launch_bounds__(NT) k_kacz_blocks(KaczBlockArgs<T> a)
     T* xis = (T*)(xb + L.xis);
     const T* bs = (const T*)(xb + L.bs);
 
-    auto project = [&](int r, int j0) {
+    // this thread's columns: thread e of a step takes row e / TPRC and the
+    // CPT columns from (e % TPRC) * CPT; NT is a multiple of TPRC, so a
+    // thread keeps its columns, shifts and relaxation in every step
+    const int j0 = (tid % TPRC) * CPT;
+    T sr[CPT], si[CPT], om[CPT];
+#pragma unroll
+    for (int k = 0; k < CPT; k++) {
+      sr[k] = a.sig_r[j0 + k];
+      si[k] = RC ? a.sig_i[j0 + k] : T(0);
+      om[k] = a.omega[j0 + k];
+    }
+    auto project = [&](int r) {
       const int e0 = lrs[r], e1 = lrs[r + 1];
       const T nrm = nds[2 * r], dg = nds[2 * r + 1];
       // the scaling does not depend on X: formed while the gathers are out
-      T f[CPT], sr[CPT], si[CPT];
+      T f[CPT];
 #pragma unroll
       for (int k = 0; k < CPT; k++) {
-        sr[k] = a.sig_r[j0 + k];
-        si[k] = RC ? a.sig_i[j0 + k] : T(0);
         T rn = nrm - T(2) * dg * sr[k] + sr[k] * sr[k];
         if (RC) rn += si[k] * si[k];
         if (rn == T(0)) rn = T(1);
-        f[k] = a.omega[j0 + k] / rn;
+        f[k] = om[k] / rn;
       }
       T tr[CPT], ti[CPT];
       const V x0 = cv_ld<T, CPT>(xs + r * TPR + j0);
@@ -310,30 +320,51 @@ __global__ void __launch_bounds__(NT) k_kacz_blocks(KaczBlockArgs<T> a)
           ti[k] = T(0);
         }
       }
-      T v[RE];
-      int c[RE];
+      if (!RC && a.distinct && e1 - e0 == RE) {
+        // RE distinct columns (every row of the honeycomb matrices): the
+        // entries and gathered values stay in registers; x_i first takes the
+        // shift term, then every entry in order (the diagonal one
+        // continuing from x_i), and each slot is stored once -- no other
+        // thread of the step touches these slots
+        T v[RE];
+        int c[RE];
+        V xg[RE];
 #pragma unroll
-      for (int q = 0; q < RE; q++) {
-        const bool in = e0 + q < e1;
-        v[q] = in ? vs[e0 + q] : T(0);
-        c[q] = in ? (int)lcs[e0 + q] : r;
-      }
-      V xg[RE], yg[RE];
-#pragma unroll
-      for (int q = 0; q < RE; q++) {
-        xg[q] = cv_ld<T, CPT>(xs + c[q] * TPR + j0);
-        if (RC) yg[q] = cv_ld<T, CPT>(xis + c[q] * TPR + j0);
-      }
-#pragma unroll
-      for (int q = 0; q < RE; q++)
-        if (e0 + q < e1) {
-#pragma unroll
-          for (int k = 0; k < CPT; k++) {
-            tr[k] += v[q] * xg[q].v[k];
-            if (RC) ti[k] += v[q] * yg[q].v[k];
-          }
+        for (int q = 0; q < RE; q++) {
+          v[q] = vs[e0 + q];
+          c[q] = lcs[e0 + q];
         }
-      for (int p = e0 + RE; p < e1; p++) {
+#pragma unroll
+        for (int q = 0; q < RE; q++) xg[q] = cv_ld<T, CPT>(xs + c[q] * TPR + j0);
+#pragma unroll
+        for (int q = 0; q < RE; q++)
+#pragma unroll
+          for (int k = 0; k < CPT; k++) tr[k] += v[q] * xg[q].v[k];
+        if (a.b) {
+          const V bb = cv_ld<T, CPT>(bs + r * TPR + j0);
+#pragma unroll
+          for (int k = 0; k < CPT; k++) tr[k] -= bb.v[k];
+        }
+        V xo = x0;
+#pragma unroll
+        for (int k = 0; k < CPT; k++) {
+          tr[k] *= f[k];
+          xo.v[k] += tr[k] * sr[k];
+        }
+#pragma unroll
+        for (int q = 0; q < RE; q++) {
+          const bool own = c[q] == r;
+          V t = own ? xo : xg[q];
+#pragma unroll
+          for (int k = 0; k < CPT; k++) t.v[k] -= tr[k] * v[q];
+          if (own) xo = t;
+          else cv_st<T, CPT>(xs + c[q] * TPR + j0, t);
+        }
+        cv_st<T, CPT>(xs + r * TPR + j0, xo);
+        return;
+      }
+      // any row: entries read from shared memory, every slot updated in place
+      for (int p = e0; p < e1; p++) {
         const T vv = vs[p];
         const int cc = lcs[p];
         const V xx = cv_ld<T, CPT>(xs + cc * TPR + j0);
@@ -355,63 +386,26 @@ __global__ void __launch_bounds__(NT) k_kacz_blocks(KaczBlockArgs<T> a)
         tr[k] *= f[k];
         if (RC) ti[k] *= f[k];
       }
-      if (a.distinct && e1 - e0 <= RE) {
-        // the row's columns are distinct and its entries are in registers:
-        // update the values gathered above (no other thread of the step
-        // touches these slots), x_i first with the shift term, then every
-        // entry in order (the diagonal one continuing from x_i), and store
-        // each slot once
-        V xo = x0, yo = y0;
-#pragma unroll
-        for (int k = 0; k < CPT; k++) {
-          if (RC) {
-            xo.v[k] += tr[k] * sr[k] + ti[k] * si[k];
-            yo.v[k] += ti[k] * sr[k] - tr[k] * si[k];
-          } else {
-            xo.v[k] += tr[k] * sr[k];
-          }
-        }
-#pragma unroll
-        for (int q = 0; q < RE; q++)
-          if (e0 + q < e1) {
-            const bool own = c[q] == r;
-            V t = own ? xo : xg[q];
-            V u;
-            if (RC) u = own ? yo : yg[q];
-#pragma unroll
-            for (int k = 0; k < CPT; k++) {
-              t.v[k] -= tr[k] * v[q];
-              if (RC) u.v[k] -= ti[k] * v[q];
-            }
-            if (own) {
-              xo = t;
-              if (RC) yo = u;
-            } else {
-              cv_st<T, CPT>(xs + c[q] * TPR + j0, t);
-              if (RC) cv_st<T, CPT>(xis + c[q] * TPR + j0, u);
-            }
-          }
-        cv_st<T, CPT>(xs + r * TPR + j0, xo);
-        if (RC) cv_st<T, CPT>(xis + r * TPR + j0, yo);
-        return;
-      }
       {
-        V x0 = cv_ld<T, CPT>(xs + r * TPR + j0);
+        // x_i was not written since it was read above
+        V xo = x0;
         if (RC) {
-          V y0 = cv_ld<T, CPT>(xis + r * TPR + j0);
+          V yo = y0;
 #pragma unroll
           for (int k = 0; k < CPT; k++) {
-            x0.v[k] += tr[k] * sr[k] + ti[k] * si[k];
-            y0.v[k] += ti[k] * sr[k] - tr[k] * si[k];
+            xo.v[k] += tr[k] * sr[k] + ti[k] * si[k];
+            yo.v[k] += ti[k] * sr[k] - tr[k] * si[k];
           }
-          cv_st<T, CPT>(xis + r * TPR + j0, y0);
+          cv_st<T, CPT>(xis + r * TPR + j0, yo);
         } else {
 #pragma unroll
-          for (int k = 0; k < CPT; k++) x0.v[k] += tr[k] * sr[k];
+          for (int k = 0; k < CPT; k++) xo.v[k] += tr[k] * sr[k];
         }
-        cv_st<T, CPT>(xs + r * TPR + j0, x0);
+        cv_st<T, CPT>(xs + r * TPR + j0, xo);
       }
-      auto scatter = [&](int cc, T vv) {
+      for (int p = e0; p < e1; p++) {
+        const T vv = vs[p];
+        const int cc = lcs[p];
         V xx = cv_ld<T, CPT>(xs + cc * TPR + j0);
 #pragma unroll
         for (int k = 0; k < CPT; k++) xx.v[k] -= tr[k] * vv;
@@ -422,18 +416,12 @@ __global__ void __launch_bounds__(NT) k_kacz_blocks(KaczBlockArgs<T> a)
           for (int k = 0; k < CPT; k++) yy.v[k] -= ti[k] * vv;
           cv_st<T, CPT>(xis + cc * TPR + j0, yy);
         }
-      };
-#pragma unroll
-      for (int q = 0; q < RE; q++)
-        if (e0 + q < e1) scatter(c[q], v[q]);
-      for (int p = e0 + RE; p < e1; p++) scatter(lcs[p], vs[p]);
+      }
     };
     auto run_step = [&](int st) {
       const int lo = sts[st], hi = sts[st + 1];
-      for (int e = tid; e < (hi - lo) * TPRC; e += NT) {
-        const int j0 = (e % TPRC) * CPT;
-        if (j0 < nv) project(lo + e / TPRC, j0);
-      }
+      if (j0 < nv)
+        for (int e = tid; e < (hi - lo) * TPRC; e += NT) project(lo + e / TPRC);
       __syncthreads();
     };
     if (a.dir & 1)
