@@ -306,6 +306,8 @@ def main():
     ap.add_argument("--nvecs", default=",".join(map(str, NVECS)))
     ap.add_argument("--no-jada", action="store_true", help="skip the eigen-solve timings")
     ap.add_argument("--no-e2e", action="store_true", help="skip the end-to-end runs through host buffers")
+    ap.add_argument("--e2e-threads", type=int, default=4,
+                    help="host threads of the end-to-end run (each on its own lane and stream)")
     ap.add_argument("--no-forms", action="store_true", help="skip the served-stream and CARP-CG timings")
     args = ap.parse_args()
     nvecs = [int(t) for t in args.nvecs.split(",")]
@@ -452,7 +454,7 @@ def main():
         hy = {k: torch.from_numpy(Y[k].get()) for k in nvecs}
     else:
         e2e_1, _, _ = e2e_run(1, args.steps)
-        e2e_2, e2e_time, hy = e2e_run(2, args.steps)
+        e2e_2, e2e_time, hy = e2e_run(max(1, args.e2e_threads), args.steps)
         e2e_time = max_over_ranks(e2e_time, dist)
         e2e_val = world * step_bytes * args.steps / e2e_time / 1e9
     ok = np.isfinite(hy[nvecs[-1]].numpy()).all()
@@ -488,9 +490,10 @@ def main():
                      "algorithmic_bytes_per_step": step_bytes},
         "e2e": {"value": None if e2e_val is None else round(e2e_val, 2), "unit": UNIT, "h2d_bytes_per_step": h2d, "d2h_bytes_per_step": d2h,
                 "path": "per block width: phist_Dmvec_set_data (pinned host X) -> phist_DsparseMat_times_mvec "
-                        "-> phist_Dmvec_get_data (pinned host Y); wall time of the timed sweeps, split over 2 "
-                        "host threads (each on its own lane/stream), so one thread's upload overlaps the "
-                        "other's download",
+                        "-> phist_Dmvec_get_data (pinned host Y); wall time of the timed sweeps, split over %d "
+                        "host threads (each on its own lane/stream), so uploads of some threads overlap "
+                        "downloads of others" % max(1, args.e2e_threads),
+                "threads": max(1, args.e2e_threads),
                 "single_thread_value": None if e2e_1 is None else round(e2e_1, 2)},
         "gpu_launches": launches,
         "clocks": clk,
