@@ -1473,10 +1473,12 @@ RowGemmArgs<T> rowgemm_args()
 // CARP
 // ======================================================================
 // Block-coloured layout (pb_carp_blocks.hpp): blocks of at most R rows
-// whose footprint has at most 2R rows of X and whose pattern at most 16R
-// entries; R is the runtime carp_block_rows, or, when that is 0, 128 for
-// sweeps of up to 8 columns, 96 up to 16 and 64 beyond (width: the number
-// of columns the sweeps are expected to have).  False when the matrix has
+// whose footprint has at most 1.25 R rows of X (at least 16; the shared
+// memory of every thread block is sized for the largest footprint, and
+// compact blocks of the benchmark matrices stay well below it) and whose
+// pattern at most 16R entries; R is the runtime carp_block_rows, or, when
+// that is 0, 128 for sweeps of up to 8 columns and 64 beyond (width: the
+// number of columns the sweeps are expected to have).  False when the matrix has
 // rows too long for that, or a block needs more than 64 steps; the caller
 // then uses the row colouring.
 template <class T>
@@ -1485,8 +1487,8 @@ bool carp_build_blocks(const SparseMat<T>* A, const std::vector<int64_t>& prp, c
 {
   const int64_t n = A->nrows;
   CarpBlocks B;
-  const int R = rt().carp_block_rows > 0 ? rt().carp_block_rows : width <= 8 ? 128 : width <= 16 ? 96 : 64;
-  if (!carp_block_partition(n, prp, pcol, R, 2 * R, 16 * R, B)) return false;
+  const int R = rt().carp_block_rows > 0 ? rt().carp_block_rows : width <= 8 ? 128 : 64;
+  if (!carp_block_partition(n, prp, pcol, R, std::max(16, R + R / 4), std::max(16, 16 * R), B)) return false;
   if (!carp_block_color(n, prp, pcol, B)) return false;
   CarpBlockLayout<T> L;
   carp_block_layout<T>(B, n, A->h_row_ptr.data(), A->h_col.data(), A->h_val.data(), L);

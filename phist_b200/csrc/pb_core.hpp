@@ -207,8 +207,8 @@ class Runtime {
   bool carp_blocks = true;
   // row limit of a block (footprint limit twice that, pattern limit 16x);
   // 0: chosen from the sweep width the work is set up for (128 rows up to 8
-  // columns, 96 up to 16, 64 beyond: the X footprint in shared memory grows
-  // with the width)
+  // columns, 64 beyond: the X footprint in shared memory grows with the
+  // width)
   int carp_block_rows = 0;
   // block sweep launches with a programmatic dependency on the previous
   // launch (overlap of its segment copies with that launch's tail)
