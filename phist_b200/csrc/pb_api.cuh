@@ -597,7 +597,7 @@ template <class T>
 void create_from_rowfunc(void** vA, const void* comm, int64_t nrows, int64_t ncols, int32_t maxnne,
                          RowFunc f, RowFuncCtor ctor, void* arg, int flags)
 {
-  PB_REQUIRE(vA && comm && f, PB_BAD_CAST, "NULL argument");
+  PB_REQUIRE(vA && f, PB_BAD_CAST, "NULL argument");  // comm NULL: the single process
   PB_REQUIRE(maxnne >= 0, PB_INVALID_INPUT, "maxnne < 0");
   std::vector<int64_t> rp(nrows + 1, 0);
   std::vector<int32_t> col;

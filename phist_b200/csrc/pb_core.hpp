@@ -94,10 +94,17 @@ void noalloc_setup_current_device();
 // Every extern "C" entry point wraps its body in PB_API_BEGIN/END: C++
 // exceptions never cross the C ABI, they become iflag codes (the reference's
 // PHIST_CHK_IERR converts exceptions to -77, src/tools/phist_macros.h:111-133).
-#define PB_API_BEGIN(iflag)        \
-  int pb_iflag_in_ = *(iflag);     \
-  (void)pb_iflag_in_;              \
-  *(iflag) = 0;                    \
+//
+// The input flag word is read once.  PHIST's flags all lie in [0, 2^14)
+// (src/kernels/phist_kernel_flags.h: the largest is PHIST_SPMVM_TASK = 8192);
+// callers that only want iflag as an output sometimes pass it uninitialised
+// (test/kernels/TestWithType_def.h:155-162, SdMatEqual, passes a fresh `int iflag`
+// to sdMat_extract_view), so a word outside that range reads as no flags.
+inline int input_flags(int w) { return (w >= 0 && w < (1 << 14)) ? w : 0; }
+#define PB_API_BEGIN(iflag)                          \
+  int pb_iflag_in_ = ::pb::input_flags(*(iflag));    \
+  (void)pb_iflag_in_;                                \
+  *(iflag) = 0;                                      \
   try {
 #define PB_API_END(iflag)                                   \
   }                                                         \

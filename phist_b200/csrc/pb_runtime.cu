@@ -355,19 +355,21 @@ void phist_comm_delete(void* comm, int* iflag)
   PB_API_END(iflag);
 }
 
+// A NULL comm is the single process, as in PHIST's builds without MPI
+// (their kernel tests never create a comm then, KernelTest.h:69-84).
 void phist_comm_get_rank(const void* comm, int* rank, int* iflag)
 {
   PB_API_BEGIN(iflag);
-  PB_REQUIRE(comm, PB_BAD_CAST, "comm is NULL");
-  *rank = ((const Comm*)comm)->rank;
+  PB_REQUIRE(rank, PB_BAD_CAST, "rank is NULL");
+  *rank = comm ? ((const Comm*)comm)->rank : 0;
   PB_API_END(iflag);
 }
 
 void phist_comm_get_size(const void* comm, int* size, int* iflag)
 {
   PB_API_BEGIN(iflag);
-  PB_REQUIRE(comm, PB_BAD_CAST, "comm is NULL");
-  *size = ((const Comm*)comm)->size;
+  PB_REQUIRE(size, PB_BAD_CAST, "size is NULL");
+  *size = comm ? ((const Comm*)comm)->size : 1;
   PB_API_END(iflag);
 }
 
@@ -382,7 +384,7 @@ void phist_comm_get_mpi_comm(const void* comm, int* mpiComm, int* iflag)
 void phist_map_create(void** map, const void* comm, int64_t nglob, int* iflag)
 {
   PB_API_BEGIN(iflag);
-  PB_REQUIRE(map && comm, PB_BAD_CAST, "map or comm is NULL");
+  PB_REQUIRE(map, PB_BAD_CAST, "map is NULL");  // comm NULL: the single process
   PB_REQUIRE(nglob >= 0 && nglob < (int64_t(1) << 31), PB_INTEGER_OVERFLOW,
              "global length %lld does not fit the 32-bit local index", (long long)nglob);
   Map* m = new Map();
