@@ -1,10 +1,12 @@
-"""PHIST's own kernel test suite, run unchanged against this library.
+"""PHIST's own test suites, run unchanged against this library.
 
 tests/phist_suite/Makefile compiles the kernel conformance tests of the
 PHIST sources (test/kernels/*.cpp with PHIST's vendored googletest) and
-links them against libphist_kernels_b200.so; the executable is built by the
-package build when the PHIST sources are present and travels with the
-built libraries.  The suite reads its test matrices from the working
+links them against libphist_kernels_b200.so; a second executable holds
+PHIST's tests of the layers above the kernels (test/core, krylov, jada,
+precon), run on PHIST's solver code compiled against this library.  The
+executables are built by the package build when the PHIST sources are
+present and travel with the built libraries.  The suite reads its test matrices from the working
 directory by name (test/tools/MatrixIO_def.hpp: D<name>.mm, S<name>.mm);
 they are written here from the golden fixture tests/golden/phist_testmats.npz
 (PHIST's test/matrices converted by tests/golden/make_golden.py), single
@@ -25,7 +27,9 @@ from conftest import GOLDEN, ROOT
 
 pytestmark = pytest.mark.gpu
 
-EXE = os.path.join(ROOT, "tests", "phist_suite", "_build", "phist_kernels_suite")
+BUILD = os.path.join(ROOT, "tests", "phist_suite", "_build")
+EXE = os.path.join(BUILD, "phist_kernels_suite")
+SOLVER_EXE = os.path.join(BUILD, "phist_solver_suite")
 
 # test (a regular expression over "Case.test") -> why it cannot pass against
 # this library
@@ -41,8 +45,12 @@ KNOWN = {
 }
 
 
-def _known(t):
-    return any(re.fullmatch(k, t) for k in KNOWN)
+# the same for PHIST's tests of the layers above the kernels
+KNOWN_SOLVER = {}
+
+
+def _known(t, known=KNOWN):
+    return any(re.fullmatch(k, t) for k in known)
 
 
 def _write_matrices(d):
@@ -59,8 +67,8 @@ def _write_matrices(d):
                     f.write("%d %d %s\n" % (i + 1, j + 1, fmt(x)))
 
 
-def _list_tests():
-    out = subprocess.run([EXE, "--gtest_list_tests"], capture_output=True, text=True, timeout=300).stdout
+def _list_tests(exe):
+    out = subprocess.run([exe, "--gtest_list_tests"], capture_output=True, text=True, timeout=300).stdout
     tests, case = [], None
     for line in out.splitlines():
         if not line.strip() or line.startswith("["):
@@ -72,12 +80,12 @@ def _list_tests():
     return tests
 
 
-def run_suite(d, log=None):
-    """runs the suite in directory d; a test that ends the process is
+def run_suite(d, log=None, exe=EXE):
+    """runs the suite exe in directory d; a test that ends the process is
     recorded and the tests not yet run are started again.  Returns
     ({test: "ok" | "failed" | "crashed" | "not run"}, number of runs)"""
     _write_matrices(d)
-    tests = [t for t in _list_tests() if ".DISABLED_" not in t and not t.startswith("DISABLED_")]
+    tests = [t for t in _list_tests(exe) if ".DISABLED_" not in t and not t.startswith("DISABLED_")]
     cases = {}
     for t in tests:
         cases.setdefault(t.split(".", 1)[0], []).append(t)
@@ -92,7 +100,7 @@ def run_suite(d, log=None):
         runs += 1
         out = os.path.join(d, "run%d.txt" % runs)
         with open(out, "w") as f:
-            r = subprocess.run(["stdbuf", "-oL", "-eL", EXE, "--gtest_filter=" + filt], cwd=d, stdout=f,
+            r = subprocess.run(["stdbuf", "-oL", "-eL", exe, "--gtest_filter=" + filt], cwd=d, stdout=f,
                                stderr=subprocess.STDOUT, timeout=2400)
         last = None
         for line in open(out, errors="replace"):
@@ -112,12 +120,20 @@ def run_suite(d, log=None):
     return result, runs
 
 
-def test_phist_kernel_suite(tmp_path):
-    if not os.path.exists(EXE):
-        pytest.skip("PHIST's kernel suite is not built (needs the PHIST sources at build time)")
-    result, runs = run_suite(str(tmp_path))
+def _check(tmp_path, exe, known, min_ran):
+    if not os.path.exists(exe):
+        pytest.skip("PHIST's test suites are not built (they need the PHIST sources at build time)")
+    result, runs = run_suite(str(tmp_path), exe=exe)
     ran = sum(v != "not run" for v in result.values())
-    bad = sorted(t for t, v in result.items() if v != "ok" and not _known(t))
-    assert ran > 1000, "only %d tests ran" % ran
-    assert not bad, "%d of %d PHIST kernel tests failed or crashed: %s" % (
+    bad = sorted(t for t, v in result.items() if v != "ok" and not _known(t, known))
+    assert ran > min_ran, "only %d tests ran" % ran
+    assert not bad, "%d of %d PHIST tests failed or crashed: %s" % (
         len(bad), ran, ", ".join("%s (%s)" % (t, result[t]) for t in bad[:40]))
+
+
+def test_phist_kernel_suite(tmp_path):
+    _check(tmp_path, EXE, KNOWN, 1000)
+
+
+def test_phist_solver_suite(tmp_path):
+    _check(tmp_path, SOLVER_EXE, KNOWN_SOLVER, 300)
