@@ -736,15 +736,35 @@ void launch_spmv_nv(const SparseMat<T>* A, const SellDev<T>& S, SpmvArgs<T>& p, 
     // resident grid, next tile's entries prefetched into shared memory
     constexpr int NT = TPR == 1 ? 128 : (TPR == 16 ? 512 : 256);
     constexpr int RPBp = NT / TPR;
-    auto kern = k_sell_spmmv_pf<T, NV, TPR, NT>;
-    static std::atomic<int> occ{0};
-    if (occ.load() == 0) {
-      int o = 0;
-      PB_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&o, kern, NT, 0));
-      occ.store(std::max(1, o));
-    }
+    // resident blocks per SM of each form, taken once
+    auto resident = [](auto kern, std::atomic<int>& occ) {
+      if (occ.load() == 0) {
+        int o = 0;
+        PB_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&o, kern, NT, 0));
+        occ.store(std::max(1, o));
+      }
+      return occ.load();
+    };
     const int64_t ntiles = ceil_div(A->nchunks, RPBp / 32);
-    const int pgrid = (int)std::max<int64_t>(1, std::min<int64_t>(ntiles, (int64_t)rt().num_sms() * occ.load()));
+    // 32-byte row segments: at least 32 bytes per thread, rows on 32-byte
+    // boundaries (vec already holds for 16 bytes)
+    constexpr int V32 = 32 / (int)sizeof(T);
+    const bool v256 = (NV / TPR) * (int)sizeof(T) >= 32 && vec && rt().spmv_v256 &&
+                      ((uintptr_t)(p.x + p.col0) & 31u) == 0 && ((uintptr_t)(p.y + p.col0) & 31u) == 0 &&
+                      p.ldx % V32 == 0 && p.ldy % V32 == 0;
+    if constexpr ((NV / TPR) * sizeof(T) >= 32) {
+      if (v256) {
+        static std::atomic<int> occ32{0};
+        auto kern = pf_kernel<T, NV, TPR, NT, false, 32>();
+        const int pgrid = (int)std::max<int64_t>(1, std::min<int64_t>(ntiles, (int64_t)rt().num_sms() * resident(kern, occ32)));
+        kern<<<pgrid, NT, 0, stream()>>>(S, p);
+        PB_LAUNCH_CHECK();
+        return;
+      }
+    }
+    static std::atomic<int> occ{0};
+    auto kern = pf_kernel<T, NV, TPR, NT>();
+    const int pgrid = (int)std::max<int64_t>(1, std::min<int64_t>(ntiles, (int64_t)rt().num_sms() * resident(kern, occ)));
     kern<<<pgrid, NT, 0, stream()>>>(S, p);
     PB_LAUNCH_CHECK();
     return;
@@ -822,7 +842,7 @@ void launch_spmv_gram_nv(const SparseMat<T>* A, SpmvArgs<T>& p, SdMat<T>* Gw, Sd
 {
   constexpr int NT = TPR == 1 ? 128 : 256;
   constexpr int RPB = NT / TPR;
-  auto kern = k_sell_spmmv_pf<T, NV, TPR, NT, true>;
+  auto kern = pf_kernel<T, NV, TPR, NT, true>();
   static std::atomic<int> occ{0};
   if (occ.load() == 0) {
     int o = 0;

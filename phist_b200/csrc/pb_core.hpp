@@ -191,7 +191,10 @@ class Runtime {
 
   // SpMMV launch shape: threads per matrix row for block widths 1,2,4,8,16,32
   // and whether the fully unrolled short-row kernel may be used
-  int spmv_tpr[6] = {1, 1, 1, 2, 4, 8};
+  // (with 256-bit gathers, 4 threads per row at width 32: two 32-byte loads
+  // per entry and thread, 8 rows of 128-byte segments per warp load, measured
+  // 273 us against 299 us for 8 threads on the L=128 Anderson matrix)
+  int spmv_tpr[6] = {1, 1, 1, 2, 4, 4};
   bool spmv_unroll = true;
   // block widths >= this use the shared-memory staged kernel (> 32: never).
   // Off by default: with one chunk per pipeline stage it measured slower
@@ -202,6 +205,12 @@ class Runtime {
   // next tile's entries prefetched into shared memory (pb_spmmv_pf.cuh);
   // false: one tile per block (pb_spmmv.cuh)
   bool spmv_pf = true;
+  // the prefetching SpMMV kernel gathers X row segments of 32 bytes or more
+  // with 256-bit loads (ld.global.v4.f64 / v8.f32) when X and Y rows start
+  // on 32-byte boundaries: half the load instructions per gathered row, and
+  // 12 / 17 / 21 % more bandwidth at widths 4 / 8 / 16 on the L=128 Anderson
+  // matrix (bitwise the same results)
+  bool spmv_v256 = true;
   // stage block-vector tiles of the Gram kernels with TMA (else cp.async)
   bool use_tma = true;
   // FP64 block products on the tensor cores (DMMA) for widths multiple of 8

@@ -46,6 +46,7 @@ void Runtime::init()
   if (const char* c = getenv("PHIST_B200_SELL_C")) sell_C = atoi(c);
   if (const char* s = getenv("PHIST_B200_SELL_SIGMA")) sell_sigma_default = atoll(s);
   if (const char* v = getenv("PHIST_B200_SPMV_PREFETCH")) spmv_pf = atoi(v) != 0;
+  if (const char* v = getenv("PHIST_B200_SPMV_V256")) spmv_v256 = atoi(v) != 0;
   if (const char* v = getenv("PHIST_B200_CARP_BLOCKS")) carp_blocks = atoi(v) != 0;
   if (const char* v = getenv("PHIST_B200_CARP_BLOCK_ROWS")) carp_block_rows = std::max(0, std::min(256, atoi(v)));
   if (const char* v = getenv("PHIST_B200_CARP_PDL")) carp_pdl = atoi(v) != 0;
@@ -558,6 +559,7 @@ void phist_b200_set_option(const char* name, int value, int* iflag)
   else if (o == "dmma") rt().use_dmma = value != 0;
   else if (o == "graphs") rt().use_graphs = value != 0;
   else if (o == "carp_blocks") rt().carp_blocks = value != 0;
+  else if (o == "spmv_v256") rt().spmv_v256 = value != 0;
   else PB_REQUIRE(false, PB_INVALID_INPUT, "unknown option '%s'", name);
   PB_API_END(iflag);
 }

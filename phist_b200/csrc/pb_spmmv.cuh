@@ -83,6 +83,50 @@ struct VecLd<double, 2> {
     *reinterpret_cast<double2*>(p) = make_double2(o[0], o[1]);
   }
 };
+// 256-bit forms (sm_100): one load or store moves 32 bytes
+template <>
+struct VecLd<double, 4> {
+  static __device__ __forceinline__ void ld(const double* p, double* o) { ld_ordered(p, o); }
+  static __device__ __forceinline__ void ld_plain(const double* p, double* o)
+  {
+    asm volatile("ld.global.v4.f64 {%0, %1, %2, %3}, [%4];\n"
+                 : "=d"(o[0]), "=d"(o[1]), "=d"(o[2]), "=d"(o[3])
+                 : "l"(p));
+  }
+  static __device__ __forceinline__ void ld_ordered(const double* p, double* o)
+  {
+    asm volatile("ld.global.nc.v4.f64 {%0, %1, %2, %3}, [%4];\n"
+                 : "=d"(o[0]), "=d"(o[1]), "=d"(o[2]), "=d"(o[3])
+                 : "l"(p));
+  }
+  static __device__ __forceinline__ void st(double* p, const double* o)
+  {
+    asm volatile("st.global.v4.f64 [%0], {%1, %2, %3, %4};\n" ::"l"(p), "d"(o[0]), "d"(o[1]), "d"(o[2]), "d"(o[3])
+                 : "memory");
+  }
+};
+template <>
+struct VecLd<float, 8> {
+  static __device__ __forceinline__ void ld(const float* p, float* o) { ld_ordered(p, o); }
+  static __device__ __forceinline__ void ld_plain(const float* p, float* o)
+  {
+    asm volatile("ld.global.v8.f32 {%0, %1, %2, %3, %4, %5, %6, %7}, [%8];\n"
+                 : "=f"(o[0]), "=f"(o[1]), "=f"(o[2]), "=f"(o[3]), "=f"(o[4]), "=f"(o[5]), "=f"(o[6]), "=f"(o[7])
+                 : "l"(p));
+  }
+  static __device__ __forceinline__ void ld_ordered(const float* p, float* o)
+  {
+    asm volatile("ld.global.nc.v8.f32 {%0, %1, %2, %3, %4, %5, %6, %7}, [%8];\n"
+                 : "=f"(o[0]), "=f"(o[1]), "=f"(o[2]), "=f"(o[3]), "=f"(o[4]), "=f"(o[5]), "=f"(o[6]), "=f"(o[7])
+                 : "l"(p));
+  }
+  static __device__ __forceinline__ void st(float* p, const float* o)
+  {
+    asm volatile("st.global.v8.f32 [%0], {%1, %2, %3, %4, %5, %6, %7, %8};\n" ::"l"(p), "f"(o[0]), "f"(o[1]),
+                 "f"(o[2]), "f"(o[3]), "f"(o[4]), "f"(o[5]), "f"(o[6]), "f"(o[7])
+                 : "memory");
+  }
+};
 template <>
 struct VecLd<float, 4> {
   static __device__ __forceinline__ void ld(const float* p, float* o)

@@ -211,12 +211,14 @@ struct GramPick<double, NV, NT, RPB> {
   typedef typename std::conditional<NV % 16 == 0, GramDmma<NV, NT, RPB>, GramScalar<double, NV, NT, RPB>>::type type;
 };
 
-template <class T, int NV, int TPR, int NT, bool GRAM = false>
-__global__ void __launch_bounds__(NT) k_sell_spmmv_pf(SellDev<T> A, SpmvArgs<T> p)
+// VB: bytes per vector load and store of an X or Y row segment (16, or 32
+// with the 256-bit forms when rows start on 32-byte boundaries)
+template <class T, int NV, int TPR, int NT, bool GRAM, int VB>
+__device__ __forceinline__ void sell_spmmv_pf(const SellDev<T>& A, const SpmvArgs<T>& p)
 {
   constexpr int KMAX = 8, CC = 32;
   constexpr int VPT = NV / TPR;
-  constexpr int VWMAX = 16 / sizeof(T);
+  constexpr int VWMAX = VB / sizeof(T);
   constexpr int VW = VPT < VWMAX ? VPT : VWMAX;
   constexpr int NVV = VPT / VW;
   constexpr int RPB = NT / TPR;        // rows per tile
@@ -407,6 +409,47 @@ __global__ void __launch_bounds__(NT) k_sell_spmmv_pf(SellDev<T> A, SpmvArgs<T> 
     __syncthreads();
   }
   if constexpr (GRAM) gram.store(p, gys);
+}
+
+// The kernel comes in two entry points around the same body: with a minimum
+// of resident blocks per SM handed to ptxas, which changes how it allocates
+// registers and schedules the gathers, and without.  pf_min_blocks is the
+// choice per form, measured on the L=128 Anderson matrix (FP64, 256-bit
+// gathers; GB/s without -> with): plain SpMMV at width 4 (1 thread per row)
+// 4,469 -> 4,748 with any minimum of 1..4, at 8 (2 per row) 4,728 -> 4,941
+// and at 16 (4 per row) 4,358 -> 4,647 with 4, at 32 best without (4,575;
+// 4,425 with 3 or 4); the single pass with W'W and V'W at widths 2 / 8 / 16
+// 2,871 -> 3,015, 2,081 -> 2,206, 1,931 -> 2,081 with 4 / 3 / 4.  The FP32
+// forms keep the plain entry point.
+template <class T, int NV, int TPR, int NT, bool GRAM>
+constexpr int pf_min_blocks()
+{
+  if (!std::is_same<T, double>::value) return 0;
+  if (!GRAM) return ((NV == 4 && TPR == 1) || (NV == 8 && TPR == 2) || (NV == 16 && TPR == 4)) ? 4 : 0;
+  return NV == 2 ? 4 : NV == 8 ? 3 : NV == 16 ? 4 : 0;
+}
+
+template <class T, int NV, int TPR, int NT, bool GRAM = false, int VB = 16>
+__global__ void __launch_bounds__(NT) k_sell_spmmv_pf(SellDev<T> A, SpmvArgs<T> p)
+{
+  sell_spmmv_pf<T, NV, TPR, NT, GRAM, VB>(A, p);
+}
+
+template <class T, int NV, int TPR, int NT, bool GRAM, int VB, int MB>
+__global__ void __launch_bounds__(NT, MB) k_sell_spmmv_pf_mb(SellDev<T> A, SpmvArgs<T> p)
+{
+  sell_spmmv_pf<T, NV, TPR, NT, GRAM, VB>(A, p);
+}
+
+// the entry point of a form
+template <class T, int NV, int TPR, int NT, bool GRAM = false, int VB = 16>
+constexpr auto pf_kernel()
+{
+  constexpr int mb = pf_min_blocks<T, NV, TPR, NT, GRAM>();
+  if constexpr (mb > 0)
+    return &k_sell_spmmv_pf_mb<T, NV, TPR, NT, GRAM, VB, mb>;
+  else
+    return &k_sell_spmmv_pf<T, NV, TPR, NT, GRAM, VB>;
 }
 
 }  // namespace pb
