@@ -448,9 +448,12 @@ void phist_b200_set_graphs(int on, int* iflag);
  * phist_b200_set_graphs, PHIST_B200_GRAPHS), "carp_blocks" (CARP sweeps
  * over a block colouring with X staged in shared memory, else one launch per
  * row colour class; PHIST_B200_CARP_BLOCKS; applies to CARP work set up
- * afterwards).  "graphs" never changes a result; tma/dmma change the
- * summation order of the block products; carp_blocks changes the row order
- * of the sweep (phist_b200_Dcarp_color_order reports it).
+ * afterwards), "spmv_v256" (SpMMV gathers X row segments of 32 bytes or
+ * more with 256-bit loads when rows start on 32-byte boundaries,
+ * PHIST_B200_SPMV_V256).  "graphs" and "spmv_v256" never change a result;
+ * tma/dmma change the summation order of the block products; carp_blocks
+ * changes the row order of the sweep (phist_b200_Dcarp_color_order reports
+ * it).
  * Unknown names: PHIST_INVALID_INPUT. */
 void phist_b200_set_option(const char* name, int value, int* iflag);
 /* SpMMV autotuner (no PHIST counterpart: GHOST fixes C = 32 on CUDA and sigma
