@@ -196,8 +196,10 @@ def jada_forms(timeout=300):
     smallest eigenpairs, block size 4, minBas 20, maxBas 40, tol 1e-10,
     start block uniform[-1,1) seed 0; the plain FP64 drop-in (PHIST's
     GMRES for the correction equations), the device-resident GMRES in FP64,
-    and FP32 correction equations on the device GMRES.  Each solve runs
-    twice in one process; the second (warm) wall time is reported."""
+    FP32 correction equations on the device GMRES, and the same two on the
+    device MINRES (innerSolvType=MINRES; the matrix is symmetric).  Each
+    solve runs twice in one process; the second (warm) wall time is
+    reported."""
     exe = os.path.join(ROOT, "phist_b200", "lib", "jada_run")
     if not os.path.exists(exe):
         return {"unavailable": "phist_b200/lib/jada_run is not built (phist_b200/solvers/Makefile)"}
@@ -205,7 +207,9 @@ def jada_forms(timeout=300):
               "which=SR", "seed=0", "reps=2"]
     forms = {}
     for name, extra in (("fp64_phist_gmres", []), ("fp64_device_gmres", ["devgmres=1"]),
-                        ("mixed_device_gmres", ["mixed=1", "devgmres=1"])):
+                        ("mixed_device_gmres", ["mixed=1", "devgmres=1"]),
+                        ("fp64_device_minres", ["devgmres=1", "innerSolvType=MINRES"]),
+                        ("mixed_device_minres", ["mixed=1", "devgmres=1", "innerSolvType=MINRES"])):
         try:
             r = subprocess.run([exe] + common + extra, capture_output=True, text=True, timeout=timeout)
             d = json.loads([ln for ln in r.stdout.splitlines() if ln.startswith("{")][-1])
@@ -250,7 +254,9 @@ def served_forms(timeout=300):
     on an L^3 grid, L log-uniform in [24, 64], through
     phist_b200/lib/serve_run (PHIST's unchanged subspacejada per request).
     Forms: plain FP64 drop-in on one stream; FP64 and FP32-correction
-    solves on the device GMRES served by 8 workers on their own lanes."""
+    solves on the device GMRES served by 8 workers on their own lanes; the
+    FP32-correction solves on the device MINRES (the matrices are
+    symmetric)."""
     exe = os.path.join(ROOT, "phist_b200", "lib", "serve_run")
     if not os.path.exists(exe):
         return {"unavailable": "phist_b200/lib/serve_run is not built (phist_b200/solvers/Makefile)"}
@@ -258,7 +264,8 @@ def served_forms(timeout=300):
     forms = {}
     for name, extra in (("fp64_one_stream", ["workers=1", "devgmres=0"]),
                         ("fp64_device_gmres_served", ["workers=8", "devgmres=1"]),
-                        ("mixed_device_gmres_served", ["workers=8", "devgmres=1", "mixed=1"])):
+                        ("mixed_device_gmres_served", ["workers=8", "devgmres=1", "mixed=1"]),
+                        ("mixed_device_minres_served", ["workers=8", "devgmres=1", "mixed=1", "minres=1"])):
         try:
             r = subprocess.run([exe] + common + extra, capture_output=True, text=True, timeout=timeout)
             d = json.loads([ln for ln in r.stdout.splitlines() if ln.startswith("{")][-1])

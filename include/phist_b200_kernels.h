@@ -419,6 +419,21 @@ void phist_b200_SjadaCorrection_gmres(phist_Sconst_sparseMat_ptr A, phist_Sconst
                                       phist_Sconst_mvec_ptr res, const int resIndex[], int k,
                                       const double sigma[], const double tol[], int maxIter, int maxBas,
                                       phist_Smvec_ptr t, int* iflag);
+/* The same solve with PHIST's blocked MINRES step (the task of
+ * jadaCorrectionSolver_run with MINRES, phist_jadaCorrectionSolver_def.hpp:
+ * 499-503; src/krylov/phist_blockedminres_def.hpp): the Lanczos three-term
+ * recurrence alpha = V_j'W, W -= alpha V_j + beta V_{j-1} in place of
+ * Gram-Schmidt, so every step costs the same; rotations, least squares,
+ * restarts and the returned t as above; converged below 100 eps absolute or
+ * tol[j] relative.  For symmetric A (real shifts), as PHIST's MINRES. */
+void phist_b200_DjadaCorrection_minres(phist_Dconst_sparseMat_ptr A, phist_Dconst_mvec_ptr Q,
+                                       phist_Dconst_mvec_ptr res, const int resIndex[], int k,
+                                       const double sigma[], const double tol[], int maxIter, int maxBas,
+                                       phist_Dmvec_ptr t, int* iflag);
+void phist_b200_SjadaCorrection_minres(phist_Sconst_sparseMat_ptr A, phist_Sconst_mvec_ptr Q,
+                                       phist_Sconst_mvec_ptr res, const int resIndex[], int k,
+                                       const double sigma[], const double tol[], int maxIter, int maxBas,
+                                       phist_Smvec_ptr t, int* iflag);
 
 /* runtime controls and statistics (library extensions) */
 /* SELL chunk height C (1..32, power of two) and the sigma window used when a

@@ -448,6 +448,81 @@ def jada_gmres(A, Q, R, sigma, tol, max_iter, max_bas, res_index=None):
     return T, conv
 
 
+def jada_minres(A, Q, R, sigma, tol, max_iter, max_bas, res_index=None):
+    """MINRES for the Jacobi-Davidson correction equations, restated in numpy
+    from PHIST's blocked MINRES as jadaCorrectionSolver_run drives it
+    (src/jada/phist_jadaCorrectionSolver_def.hpp:499-503,
+    src/krylov/phist_blockedminres_def.hpp:185-277): per system s, operator
+    P (A - sigma_s I) with P = I - Q Q', x_0 = 0, the Lanczos recurrence
+    w = op v_j, alpha = v_j'w, w -= alpha v_j, w -= beta v_{j-1} (beta the
+    previous norm), beta' = ||w||, H tridiagonal; the basis kept, Givens
+    rotations and least squares as in jada_gmres; convergence when the
+    residual estimate is below 100 eps or tol_s * ||b_s||
+    (blockedminres_def.hpp:157), restart after max_bas steps, at most
+    max_iter steps, the solutions scaled to unit norm.  A: dense symmetric
+    n x n.  Returns (t, converged flags)."""
+    A = np.asarray(A, np.float64)
+    n = A.shape[0]
+    k = len(sigma)
+    P = np.eye(n) - (Q @ Q.T if Q is not None and Q.shape[1] else 0.0)
+    eps = 100 * np.finfo(np.float64).eps
+    T = np.zeros((n, k))
+    conv = np.zeros(k, bool)
+    m = max(1, min(max_bas if max_bas > 0 else max_iter, max_iter, 63))
+    for s in range(k):
+        b = R[:, res_index[s] if res_index is not None else s].astype(np.float64)
+        op = P @ (A - sigma[s] * np.eye(n))
+        x = np.zeros(n)
+        bnorm = np.linalg.norm(b)
+        done = bnorm < eps
+        total = 0
+        while total < max_iter and not done:
+            r = b - op @ x
+            beta = np.linalg.norm(r)
+            V = np.zeros((n, m + 1))
+            H = np.zeros((m + 1, m))
+            cs, sn = np.zeros(m), np.zeros(m)
+            g = np.zeros(m + 1)
+            g[0] = beta
+            V[:, 0] = r / beta if beta > 0 else 0.0
+            jc = 0
+            bprev = 0.0
+            for j in range(min(m, max_iter - total)):
+                w = op @ V[:, j]
+                alpha = V[:, j] @ w
+                w = w - alpha * V[:, j]
+                if j > 0:
+                    w = w - bprev * V[:, j - 1]
+                    H[j - 1, j] = bprev
+                H[j, j] = alpha
+                hn = np.linalg.norm(w)
+                bprev = hn
+                V[:, j + 1] = w / hn if hn > 0 else 0.0
+                for i in range(j):
+                    a, bb = H[i, j], H[i + 1, j]
+                    H[i, j], H[i + 1, j] = cs[i] * a + sn[i] * bb, -sn[i] * a + cs[i] * bb
+                a = H[j, j]
+                rr = np.hypot(a, hn)
+                c, sg = (a / rr, hn / rr) if rr > 0 else (1.0, 0.0)
+                cs[j], sn[j] = c, sg
+                H[j, j] = rr
+                g[j], g[j + 1] = c * g[j], -sg * g[j]
+                jc = j + 1
+                res = abs(g[j + 1])
+                if res < eps or (bnorm > 0 and res / bnorm < tol[s]):
+                    done = True
+                    break
+            y = np.zeros(jc)
+            for i in range(jc - 1, -1, -1):
+                y[i] = (g[i] - H[i, i + 1:jc] @ y[i + 1:jc]) / H[i, i] if H[i, i] != 0 else 0.0
+            x = x + V[:, :jc] @ y
+            total += jc
+        nx = np.linalg.norm(x)
+        T[:, s] = x / nx if nx > 0 else 0.0
+        conv[s] = done
+    return T, conv
+
+
 def carp_cgmn(rowptr, col, val, sigma, b, iters, order=None):
     """CGMN (CARP-CG) for the shifted systems (A - sigma_j I) x_j = b_j, one
     per column, restated from PHIST's carp_cg

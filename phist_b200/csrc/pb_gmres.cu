@@ -24,6 +24,17 @@
 // current iterate; at most maxIter steps in all; the solutions returned with
 // unit norm (phist_jadaCorrectionSolver_def.hpp:576-578).  The small dense
 // part (Hessenberg, rotations, triangular solve) is FP64 in both precisions.
+//
+// MINRES (phist_b200_{D,S}jadaCorrection_minres) is the same solver with
+// PHIST's blocked MINRES step (src/krylov/phist_blockedminres_def.hpp:
+// 185-277) in place of the Gram-Schmidt step: the Lanczos three-term
+// recurrence alpha = V_j'W, W -= alpha V_j + beta V_{j-1} with beta the
+// previous step's norm, beta' = ||W||, so H is tridiagonal and a step costs
+// two passes over W whatever its index; the basis is kept (PHIST's ring
+// buffer) for the update of the iterate, the rotations, least squares and
+// restarts are GMRES's, and the absolute threshold is 100 eps
+// (blockedminres_def.hpp:157).  For symmetric A and real shifts only, as in
+// PHIST.
 #include <algorithm>
 #include <atomic>
 #include <cmath>
@@ -310,6 +321,27 @@ __global__ void k_gm_decide(const T* __restrict__ O1, const T* __restrict__ O2, 
   if (s == 0) *reorth = any;
 }
 
+// Lanczos step j (MINRES): alpha_s = V_j'w_s from the dots at O1 + j*k,
+// beta_s = the previous step's unrotated norm h(j, j-1) = sqrt(Nf_s) (read
+// before this step's update overwrites Nf); column j of H is 0 above j-1,
+// beta at j-1, alpha at j, and the update coefficients of V_{j-1}, V_j are
+// hL[(j-1)*k + s] = beta, hL[j*k + s] = alpha
+template <class T>
+__global__ void k_lz_coef(const T* __restrict__ O1, const T* __restrict__ Nf, int j, int k, int m, double* H, T* hL)
+{
+  const int s = threadIdx.x;
+  if (s >= k) return;
+  const double alpha = (double)O1[j * k + s];
+  const double beta = j > 0 ? sqrt(fmax((double)Nf[s], 0.0)) : 0.0;
+  for (int i = 0; i + 1 < j; i++) H[((int64_t)i * m + j) * k + s] = 0.0;
+  if (j > 0) {
+    H[((int64_t)(j - 1) * m + j) * k + s] = beta;
+    hL[(j - 1) * k + s] = (T)beta;
+  }
+  H[((int64_t)j * m + j) * k + s] = alpha;
+  hL[j * k + s] = (T)alpha;
+}
+
 // out[o] = sum over blocks of part[b*nout + o] (k_reduce_partials) unless
 // *skip == 0
 template <class T>
@@ -410,9 +442,10 @@ static void gm_mvsd(int64_t n, int m, int k, T alpha, const T* V, int64_t ldv, c
   launch_rowgemm<T>(a);
 }
 
+// lanczos: MINRES (three-term recurrence), else GMRES
 template <class T>
-int jada_gmres(const SparseMat<T>* A, const Mvec<T>* Q, const Mvec<T>* R, const int* resIndex, int k,
-               const double* sigma, const double* tol, int maxIter, int maxBas, Mvec<T>* t)
+int jada_krylov(const SparseMat<T>* A, const Mvec<T>* Q, const Mvec<T>* R, const int* resIndex, int k,
+                const double* sigma, const double* tol, int maxIter, int maxBas, Mvec<T>* t, bool lanczos)
 {
   PB_REQUIRE(A && R && t && sigma && tol, PB_INVALID_INPUT, "NULL argument");
   PB_REQUIRE(k >= 1 && k <= 32, PB_INVALID_INPUT, "1..32 systems per call (got %d)", k);
@@ -428,14 +461,14 @@ int jada_gmres(const SparseMat<T>* A, const Mvec<T>* Q, const Mvec<T>* R, const 
   const int nq = Q ? Q->nvec : 0;
   const int m = std::max(1, std::min(std::min(maxBas > 0 ? maxBas : maxIter, maxIter), 63));
   const int64_t nk = n * (int64_t)k;  // one basis block
-  const double eps_abs = 1000.0 * std::numeric_limits<T>::epsilon();
+  const double eps_abs = (lanczos ? 100.0 : 1000.0) * std::numeric_limits<T>::epsilon();
 
   DBuf<T> V((size_t)nk * (m + 1)), B((size_t)nk), X((size_t)nk), W((size_t)nk);
   DBuf<T> Y((size_t)(m + 1) * k), Cq((size_t)std::max(nq, 1) * k), dummy(k);
   DBuf<T> Gk((size_t)k * k), f(k);
   DBuf<double> H((size_t)(m + 1) * m * k), cs((size_t)m * k), sn((size_t)m * k), g((size_t)(m + 1) * k), bnorm(k);
   DBuf<int> conv(k), jcount(k), reorth(1);
-  DBuf<T> O1((size_t)(m + 2) * k), O2((size_t)(m + 2) * k), Nf(k);
+  DBuf<T> O1((size_t)(m + 2) * k), O2((size_t)(m + 2) * k), Nf(k), hL((size_t)(m + 1) * k);
   GmIndex gi;
   GmTol gt;
   for (int s = 0; s < k; s++) {
@@ -500,17 +533,25 @@ int jada_gmres(const SparseMat<T>* A, const Mvec<T>* Q, const Mvec<T>* R, const 
       // below 1/sqrt(2) of its value before (a device flag the second-pass
       // kernels read)
       const int J = j + 1;
-      if (J <= gm_chunk(k)) {
-        gm_blk<T, false, true>(n, k, 0, J, V.p, W.p, nullptr, nullptr, O1.p);
-        gm_blk<T, true, true>(n, k, 0, J, V.p, W.p, O1.p, nullptr, O2.p);
+      if (lanczos) {
+        // alpha = V_j'W; W -= V_{j-1} beta + V_j alpha and ||W||^2 into Nf
+        gm_blk<T, false, true>(n, k, j, J, V.p, W.p, nullptr, nullptr, O1.p);
+        k_lz_coef<T><<<1, 32, 0, stream()>>>(O1.p, Nf.p, j, k, m, H.p, hL.p);
+        PB_LAUNCH_CHECK();
+        gm_blk<T, true, false>(n, k, std::max(0, j - 1), J, V.p, W.p, hL.p, nullptr, Nf.p);
       } else {
-        gm_dots<T>(n, k, J, V.p, W.p, O1.p);
-        gm_update<T>(n, k, J, V.p, W.p, O1.p, nullptr, dummy.p);
-        gm_dots<T>(n, k, J, V.p, W.p, O2.p);
+        if (J <= gm_chunk(k)) {
+          gm_blk<T, false, true>(n, k, 0, J, V.p, W.p, nullptr, nullptr, O1.p);
+          gm_blk<T, true, true>(n, k, 0, J, V.p, W.p, O1.p, nullptr, O2.p);
+        } else {
+          gm_dots<T>(n, k, J, V.p, W.p, O1.p);
+          gm_update<T>(n, k, J, V.p, W.p, O1.p, nullptr, dummy.p);
+          gm_dots<T>(n, k, J, V.p, W.p, O2.p);
+        }
+        k_gm_decide<T><<<1, 32, 0, stream()>>>(O1.p, O2.p, J, k, m, j, H.p, Nf.p, reorth.p);
+        PB_LAUNCH_CHECK();
+        gm_update<T>(n, k, J, V.p, W.p, O2.p, reorth.p, Nf.p);
       }
-      k_gm_decide<T><<<1, 32, 0, stream()>>>(O1.p, O2.p, J, k, m, j, H.p, Nf.p, reorth.p);
-      PB_LAUNCH_CHECK();
-      gm_update<T>(n, k, J, V.p, W.p, O2.p, reorth.p, Nf.p);
       const T* nrm_p = Nf.p;
       const int nrm_stride = 1;
       k_gm_step<T><<<1, 32, 0, stream()>>>(nrm_p, nrm_stride, j, k, m, H.p, cs.p, sn.p, g.p, bnorm.p, f.p, conv.p,
@@ -547,10 +588,27 @@ int jada_gmres(const SparseMat<T>* A, const Mvec<T>* Q, const Mvec<T>* R, const 
   return unconverged;
 }
 
+template <class T>
+int jada_gmres(const SparseMat<T>* A, const Mvec<T>* Q, const Mvec<T>* R, const int* resIndex, int k,
+               const double* sigma, const double* tol, int maxIter, int maxBas, Mvec<T>* t)
+{
+  return jada_krylov<T>(A, Q, R, resIndex, k, sigma, tol, maxIter, maxBas, t, false);
+}
+template <class T>
+int jada_minres(const SparseMat<T>* A, const Mvec<T>* Q, const Mvec<T>* R, const int* resIndex, int k,
+                const double* sigma, const double* tol, int maxIter, int maxBas, Mvec<T>* t)
+{
+  return jada_krylov<T>(A, Q, R, resIndex, k, sigma, tol, maxIter, maxBas, t, true);
+}
+
 template int jada_gmres<double>(const SparseMat<double>*, const Mvec<double>*, const Mvec<double>*, const int*, int,
                                 const double*, const double*, int, int, Mvec<double>*);
 template int jada_gmres<float>(const SparseMat<float>*, const Mvec<float>*, const Mvec<float>*, const int*, int,
                                const double*, const double*, int, int, Mvec<float>*);
+template int jada_minres<double>(const SparseMat<double>*, const Mvec<double>*, const Mvec<double>*, const int*, int,
+                                 const double*, const double*, int, int, Mvec<double>*);
+template int jada_minres<float>(const SparseMat<float>*, const Mvec<float>*, const Mvec<float>*, const int*, int,
+                                const double*, const double*, int, int, Mvec<float>*);
 
 }  // namespace pb
 
@@ -574,6 +632,28 @@ void phist_b200_SjadaCorrection_gmres(const void* A, const void* Q, const void* 
   PB_API_BEGIN(iflag);
   const int u = pb::jada_gmres<float>(pb::SP<float>(A), Q ? pb::MV<float>(Q) : nullptr, pb::MV<float>(res),
                                       resIndex, k, sigma, tol, maxIter, maxBas, pb::MV<float>(t));
+  *iflag = u;
+  PB_API_END(iflag);
+}
+
+void phist_b200_DjadaCorrection_minres(const void* A, const void* Q, const void* res, const int* resIndex, int k,
+                                       const double* sigma, const double* tol, int maxIter, int maxBas, void* t,
+                                       int* iflag)
+{
+  PB_API_BEGIN(iflag);
+  const int u = pb::jada_minres<double>(pb::SP<double>(A), Q ? pb::MV<double>(Q) : nullptr, pb::MV<double>(res),
+                                        resIndex, k, sigma, tol, maxIter, maxBas, pb::MV<double>(t));
+  *iflag = u;
+  PB_API_END(iflag);
+}
+
+void phist_b200_SjadaCorrection_minres(const void* A, const void* Q, const void* res, const int* resIndex, int k,
+                                       const double* sigma, const double* tol, int maxIter, int maxBas, void* t,
+                                       int* iflag)
+{
+  PB_API_BEGIN(iflag);
+  const int u = pb::jada_minres<float>(pb::SP<float>(A), Q ? pb::MV<float>(Q) : nullptr, pb::MV<float>(res),
+                                       resIndex, k, sigma, tol, maxIter, maxBas, pb::MV<float>(t));
   *iflag = u;
   PB_API_END(iflag);
 }

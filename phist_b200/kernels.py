@@ -166,6 +166,7 @@ for _P, _ST in (("D", _ct.c_double), ("S", _ct.c_float)):
                                    _ct.POINTER(_ct.c_int64), vp, c_int_p])
     _d(x + "sparseMat_autotune", [vp, c_int, vp, c_int, vp, c_int_p])
     _d(x + "jadaCorrection_gmres", [vp, vp, vp, vp, c_int, vp, vp, c_int, c_int, vp, c_int_p])
+    _d(x + "jadaCorrection_minres", [vp, vp, vp, vp, c_int, vp, vp, c_int, c_int, vp, c_int_p])
     _d(x + "sparseMat_get_tuning", [vp, c_int_p, _ct.POINTER(_ct.c_int64), vp, vp, vp, c_int_p])
     _d(p + "mvec_create", [vpp, vp, c_int, c_int_p])
     _d(p + "mvec_clone_shape", [vpp, vp, c_int_p])

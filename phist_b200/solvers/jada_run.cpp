@@ -19,7 +19,8 @@
 //         outer iteration, Rayleigh-Ritz, orthogonalisation and residuals
 //         stay FP64)
 //         devgmres=1 (correction equations on the library's device-resident
-//         GMRES, FP64, or FP32 with mixed=1)
+//         GMRES, FP64, or FP32 with mixed=1; its MINRES with
+//         innerSolvType=MINRES)
 #include <chrono>
 #include <cmath>
 #include <cstdio>

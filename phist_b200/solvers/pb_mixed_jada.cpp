@@ -28,6 +28,12 @@ void phist_b200_DjadaCorrection_gmres(phist_Dconst_sparseMat_ptr A, phist_Dconst
 void phist_b200_SjadaCorrection_gmres(phist_Sconst_sparseMat_ptr A, phist_Sconst_mvec_ptr Q,
                                       phist_Sconst_mvec_ptr res, const int resIndex[], int k, const double sigma[],
                                       const double tol[], int maxIter, int maxBas, phist_Smvec_ptr t, int* iflag);
+void phist_b200_DjadaCorrection_minres(phist_Dconst_sparseMat_ptr A, phist_Dconst_mvec_ptr Q,
+                                       phist_Dconst_mvec_ptr res, const int resIndex[], int k, const double sigma[],
+                                       const double tol[], int maxIter, int maxBas, phist_Dmvec_ptr t, int* iflag);
+void phist_b200_SjadaCorrection_minres(phist_Sconst_sparseMat_ptr A, phist_Sconst_mvec_ptr Q,
+                                       phist_Sconst_mvec_ptr res, const int resIndex[], int k, const double sigma[],
+                                       const double tol[], int maxIter, int maxBas, phist_Smvec_ptr t, int* iflag);
 void phist_b200_mvec_DtoS(phist_Dconst_mvec_ptr X, phist_Smvec_ptr Y, int* iflag);
 void phist_b200_mvec_StoD(phist_Sconst_mvec_ptr X, phist_Dmvec_ptr Y, int* iflag);
 void phist_b200_sparseMat_DtoS(phist_Dconst_sparseMat_ptr A, phist_SsparseMat_ptr* As, int* iflag);
@@ -68,6 +74,7 @@ struct WorkBlock {
 struct pb_mixed_jada {
   int fp32 = 1;         // correction equations in FP32 (else FP64)
   int devgmres = 0;     // the library's device-resident GMRES (else PHIST's blocked GMRES)
+  int minres = 0;       // innerSolvType MINRES: the device solver runs MINRES
   int maxBas = 20;      // GMRES basis size of the device solver
   phist_Dconst_sparseMat_ptr A = nullptr;
   phist_SsparseMat_ptr As = nullptr;
@@ -114,8 +121,9 @@ static void pb_mixed_jada_run(void* data, void const* A_op, void const* B_op, vo
   if (!me->fp32) {
     // FP64 on the device-resident GMRES: no conversions
     *iflag = 0;
-    phist_b200_DjadaCorrection_gmres(me->A, (phist_Dconst_mvec_ptr)Qtil, (phist_Dconst_mvec_ptr)res, resIndex, k,
-                                     sigma_r, tol, maxIter, me->maxBas, (phist_Dmvec_ptr)t, iflag);
+    (me->minres ? phist_b200_DjadaCorrection_minres : phist_b200_DjadaCorrection_gmres)(
+        me->A, (phist_Dconst_mvec_ptr)Qtil, (phist_Dconst_mvec_ptr)res, resIndex, k, sigma_r, tol, maxIter,
+        me->maxBas, (phist_Dmvec_ptr)t, iflag);
     if (*iflag < 0) return;
     me->calls++;
     me->systems += k;
@@ -145,8 +153,8 @@ static void pb_mixed_jada_run(void* data, void const* A_op, void const* B_op, vo
 
   *iflag = 0;
   if (me->devgmres) {
-    phist_b200_SjadaCorrection_gmres(me->As, me->Q.v, me->R.v, resIndex, k, sigma_r, tol, maxIter, me->maxBas,
-                                      me->T.v, iflag);
+    (me->minres ? phist_b200_SjadaCorrection_minres : phist_b200_SjadaCorrection_gmres)(
+        me->As, me->Q.v, me->R.v, resIndex, k, sigma_r, tol, maxIter, me->maxBas, me->T.v, iflag);
   } else {
     float s[64], tl[64];
     for (int j = 0; j < k; j++) {
@@ -190,6 +198,7 @@ extern "C" void phist_b200_jada_inner_create(pb_mixed_jada** out, void const* A,
   }
   me->fp32 = fp32 ? 1 : 0;
   me->devgmres = (devgmres || !fp32) ? 1 : 0;  // FP64 here means the device GMRES
+  me->minres = opts->innerSolvType == phist_MINRES ? 1 : 0;
   me->maxBas = opts->innerSolvMaxBas > 0 ? opts->innerSolvMaxBas : opts->innerSolvMaxIters;
   me->A = (phist_Dconst_sparseMat_ptr)A;
   if (!me->fp32) {

@@ -47,7 +47,10 @@ void phist_b200_mixed_jada_create(pb_mixed_jada** me, void const* A, const phist
  * Hessenberg matrix, rotations and every dot product on the GPU, CGS2 as
  * block products, no host synchronisation per step) instead of PHIST's
  * blocked GMRES.  fp32 = 0 always means the device GMRES (PHIST's own FP64
- * GMRES is what subspacejada runs without this hook).  GMRES basis size:
+ * GMRES is what subspacejada runs without this hook).  With innerSolvType
+ * MINRES the device solver runs MINRES instead
+ * (phist_b200_{D,S}jadaCorrection_minres: the Lanczos three-term recurrence
+ * of PHIST's blocked MINRES, for symmetric A).  Basis size:
  * innerSolvMaxBas, or innerSolvMaxIters when that is < 0 (PHIST's rule,
  * src/jada/phist_jadaCorrectionSolver_def.hpp:37-38). */
 void phist_b200_jada_inner_create(pb_mixed_jada** me, void const* A, const phist_jadaOpts* opts, int fp32,

@@ -20,7 +20,9 @@
 //         numEigs (8) blockSize (4) minBas (16) maxBas (32) tol (1e-10)
 //         maxIters (400) mixed (0: FP64; 1: FP32 correction equations,
 //         pb_mixed_jada.h) devgmres (1: correction equations on the
-//         library's device-resident GMRES) budget_frac (0.8)
+//         library's device-resident GMRES) minres (1: MINRES for the
+//         correction equations, on the device with devgmres=1; the served
+//         matrices are symmetric) budget_frac (0.8)
 //         only=<i> : serve request i alone (arrival at once), for checking
 //                    that a result is the same alone and in the mix
 // Output: one JSON line with per-request latency (completion - arrival),
@@ -84,7 +86,7 @@ struct Result {
 };
 
 struct Opts {
-  int numEigs = 8, blockSize = 4, minBas = 16, maxBas = 32, maxIters = 400, mixed = 0, devgmres = 0;
+  int numEigs = 8, blockSize = 4, minBas = 16, maxBas = 32, maxIters = 400, mixed = 0, devgmres = 0, minres = 0;
   double tol = 1e-10;
 };
 
@@ -129,7 +131,7 @@ void solve(const Request& q, const Opts& o, phist_const_comm_ptr comm, Result& r
   opts.maxBas = o.maxBas;
   opts.convTol = o.tol;
   opts.maxIters = o.maxIters;
-  opts.innerSolvType = phist_GMRES;
+  opts.innerSolvType = o.minres ? phist_MINRES : phist_GMRES;
   opts.innerSolvMaxIters = 20;
   opts.symmetry = phist_HERMITIAN;
   pb_mixed_jada* mj = NULL;
@@ -224,6 +226,7 @@ int main(int argc, char** argv)
     else if (k == "maxIters") o.maxIters = atoi(v);
     else if (k == "mixed") o.mixed = atoi(v);
     else if (k == "devgmres") o.devgmres = atoi(v);
+    else if (k == "minres") o.minres = atoi(v);
     else if (k == "budget_frac") budget_frac = atof(v);
     else if (k == "only") only = atoi(v);
   }
@@ -314,11 +317,11 @@ int main(int argc, char** argv)
   }
   int nlanes = 0;
   phist_b200_lane_count(&nlanes, &iflag);
-  printf("{\"served\": %d, \"workers\": %d, \"mixed\": %d, \"devgmres\": %d, \"rate\": %g, \"seed\": %llu, \"numEigs\": %d, "
+  printf("{\"served\": %d, \"workers\": %d, \"mixed\": %d, \"devgmres\": %d, \"minres\": %d, \"rate\": %g, \"seed\": %llu, \"numEigs\": %d, "
          "\"tol\": %.1e, \"failed\": %d, \"unconverged\": %d, \"max_resExplicit\": %.3e, \"wall\": %.4f, "
          "\"solves_per_s\": %.4f, \"latency_p50\": %.4f, \"latency_p99\": %.4f, \"latency_mean\": %.4f, "
          "\"max_concurrent\": %d, \"lanes\": %d, \"budget_GB\": %.2f, \"peak_admitted_GB\": %.3f, \"requests\": [",
-         (int)order.size(), workers, o.mixed, o.devgmres, rate, (unsigned long long)seed, o.numEigs, o.tol, failed, unconverged,
+         (int)order.size(), workers, o.mixed, o.devgmres, o.minres, rate, (unsigned long long)seed, o.numEigs, o.tol, failed, unconverged,
          maxres, wall, order.size() / std::max(1e-9, last_end - first_arr), percentile(lat, 0.5),
          percentile(lat, 0.99), [&] { double s = 0; for (double x : lat) s += x; return s / lat.size(); }(),
          max_concurrent, nlanes, budget / 1e9, peak_inflight / 1e9);

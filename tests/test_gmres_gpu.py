@@ -1,8 +1,10 @@
-"""Device-resident GMRES for the Jacobi-Davidson correction equations
-(phist_b200_{D,S}jadaCorrection_gmres, csrc/pb_gmres.cu) against the numpy
-restatement of PHIST's GMRES in the oracle: the GMRES iterate after a given
-number of steps is unique (the residual minimiser over the Krylov space), so
-cut-off runs, restarted runs and converged runs must agree with it."""
+"""Device-resident GMRES and MINRES for the Jacobi-Davidson correction
+equations (phist_b200_{D,S}jadaCorrection_{gmres,minres}, csrc/pb_gmres.cu)
+against the numpy restatements of PHIST's GMRES and MINRES in the oracle: the
+iterate after a given number of steps is unique (the residual minimiser over
+the Krylov space), so cut-off runs, restarted runs and converged runs must
+agree with it.  For the symmetric test operators MINRES and GMRES minimise
+over the same space, so the MINRES iterate also equals GMRES's."""
 import numpy as np
 import pytest
 
@@ -30,7 +32,7 @@ def _setup(problem, nq, k, seed, extra=0):
     return rp, c, v, Q, R, sigma
 
 
-def _run(rp, c, v, Q, R, sigma, tol, max_iter, max_bas, res_index=None, dtype=np.float64):
+def _run(rp, c, v, Q, R, sigma, tol, max_iter, max_bas, res_index=None, dtype=np.float64, solver="gmres"):
     from phist_b200 import kernels as K
     from phist_b200.objects import Mvec, SparseMat
     A = SparseMat.from_crs(rp, c, v, dtype=dtype)
@@ -41,7 +43,7 @@ def _run(rp, c, v, Q, R, sigma, tol, max_iter, max_bas, res_index=None, dtype=np
     sg = np.ascontiguousarray(sigma, np.float64)
     tl = np.full(k, tol, np.float64)
     idx = np.ascontiguousarray(res_index, np.int32) if res_index is not None else None
-    f = K.phist_b200_DjadaCorrection_gmres if dtype == np.float64 else K.phist_b200_SjadaCorrection_gmres
+    f = getattr(K, "phist_b200_%sjadaCorrection_%s" % ("D" if dtype == np.float64 else "S", solver))
     iflag = K.iflag_of(f, A.h, Qm.h if Qm else None, Rm.h, K.ptr(idx) if idx is not None else None, k, K.ptr(sg),
                        K.ptr(tl), max_iter, max_bas, Tm.h)
     t = Tm.get()
@@ -118,3 +120,60 @@ def test_gmres_bad_arguments(session):
                       T.h) < 0
     for o in (R, T, A):
         o.delete()
+
+
+# symmetric problems only (PHIST's MINRES needs a symmetric operator)
+@pytest.mark.parametrize("problem,nq,k,max_iter,max_bas", [("LAPDIAG3D-8-S1", 6, 4, 7, 20),
+                                                           ("LAPDIAG3D-8-S1", 6, 4, 12, 4),
+                                                           ("LAPLACE3D-7", 0, 3, 10, 20),
+                                                           ("LAPDIAG3D-9-S4", 4, 4, 16, 16),
+                                                           ("LAPDIAG3D-8-S1", 2, 8, 10, 10)])
+def test_minres_cut_off_matches_oracle(session, oracle, problem, nq, k, max_iter, max_bas):
+    """no convergence within max_iter: the MINRES iterate of exactly max_iter
+    steps (restarts every max_bas), against the oracle's MINRES and GMRES"""
+    rp, c, v, Q, R, sigma = _setup(problem, nq, k, 3)
+    t, iflag = _run(rp, c, v, Q, R, sigma, 1e-30, max_iter, max_bas, solver="minres")
+    A = _dense(rp, c, v)
+    ref, conv = oracle.jada_minres(A, Q, R, sigma, np.full(k, 1e-30), max_iter, max_bas)
+    gm, _ = oracle.jada_gmres(A, Q, R, sigma, np.full(k, 1e-30), max_iter, max_bas)
+    assert iflag == k and not conv.any()
+    assert np.abs(np.linalg.norm(t, axis=0) - 1).max() < 1e-12
+    assert relerr(t, ref) < 1e-9, relerr(t, ref)
+    assert relerr(t, gm) < 1e-7, relerr(t, gm)
+
+
+def test_minres_converges_and_res_index(session, oracle):
+    """converged systems (tolerance 1e-9), right-hand sides picked by resIndex
+    from a wider block; each t solves its system up to its scale"""
+    rp, c, v, Q, R, sigma = _setup("LAPDIAG3D-9-S2", 5, 3, 4, extra=2)
+    idx = [4, 0, 2]
+    t, iflag = _run(rp, c, v, Q, R, sigma, 1e-9, 400, 40, res_index=idx, solver="minres")
+    A = _dense(rp, c, v)
+    ref, conv = oracle.jada_minres(A, Q, R, sigma, np.full(3, 1e-9), 400, 40, res_index=idx)
+    assert iflag == 0 and conv.all()
+    assert relerr(t, ref) < 1e-6
+    P = np.eye(len(A)) - Q @ Q.T
+    for s in range(3):
+        b = R[:, idx[s]]
+        y = P @ (A - sigma[s] * np.eye(len(A))) @ t[:, s]
+        a = (y @ b) / (y @ y)
+        assert np.linalg.norm(a * y - b) / np.linalg.norm(b) < 1e-8
+
+
+def test_minres_fp32(session, oracle):
+    """the FP32 form against the FP64 oracle: agreement to FP32 rounding.
+    FP32 Lanczos loses orthogonality sooner: with restarts after 40 steps one
+    of these systems stalls above 1e-5 (so does the restatement run in FP32),
+    with the largest basis (63) all converge"""
+    rp, c, v, Q, R, sigma = _setup("LAPDIAG3D-8-S1", 6, 4, 5)
+    R *= 1024.0 / np.linalg.norm(R, axis=0)
+    t, iflag = _run(rp, c, v, Q, R, sigma, 1e-5, 400, 63, dtype=np.float32, solver="minres")
+    A = _dense(rp, c, v)
+    ref, conv = oracle.jada_minres(A, Q, R, sigma, np.full(4, 1e-5), 400, 63)
+    assert iflag == 0 and conv.all()
+    assert relerr(t, ref) < 1e-3
+    P = np.eye(len(A)) - Q @ Q.T
+    for s in range(4):
+        y = P @ (A - sigma[s] * np.eye(len(A))) @ t[:, s].astype(np.float64)
+        a = (y @ R[:, s]) / (y @ y)
+        assert np.linalg.norm(a * y - R[:, s]) / np.linalg.norm(R[:, s]) < 1e-4

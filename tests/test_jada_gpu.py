@@ -171,3 +171,27 @@ def test_subspacejada_device_gmres(session, L):
         assert max(r["resExplicit"][:10]) < 20 * tol
     assert rd["nIter"] <= 1.1 * r64["nIter"] + 2, (rd["nIter"], r64["nIter"])
     assert rm["nIter"] <= 1.5 * r64["nIter"] + 5, (rm["nIter"], r64["nIter"])
+
+
+@pytest.mark.parametrize("L", [12, 16])
+def test_subspacejada_device_minres(session, L):
+    """innerSolvType=MINRES with the device solver: the correction equations
+    on the library's device MINRES (FP64, and FP32 with mixed=1); the same 10
+    smallest eigenpairs of the symmetric problem to the same tolerance, FP64
+    within 10 % (+2) of the outer iterations of PHIST's own MINRES (host
+    Lanczos on this library's kernels)"""
+    tol, seed = 1e-10, 3
+    args = ["LAPDIAG3D-%d-S%d" % (L, seed), "numEigs=10", "blockSize=4", "minBas=20", "maxBas=40",
+            "convTol=%g" % tol, "which=SR", "innerSolvType=MINRES"]
+    rp = run(*args)
+    rd = run(*(args + ["devgmres=1"]))
+    rm = run(*(args + ["devgmres=1", "mixed=1"]))
+    exact, rho = lapdiag_eigs(L, seed, 10)
+    for r in (rp, rd, rm):
+        assert r["nConv"] >= 10
+        assert np.abs(np.sort(r["ev"][:10]) - exact).max() <= tol * rho, (r["mixed"], r["ev"][:10], exact)
+        assert max(r["resExplicit"][:10]) < 20 * tol
+    for r in (rd, rm):
+        assert r["devgmres"] == 1 and r["inner_calls"] > 0
+    assert rd["nIter"] <= 1.1 * rp["nIter"] + 2, (rd["nIter"], rp["nIter"])
+    assert rm["nIter"] <= 1.5 * rp["nIter"] + 5, (rm["nIter"], rp["nIter"])

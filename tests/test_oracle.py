@@ -281,6 +281,38 @@ def test_oracle_jada_gmres_restart_semantics():
     assert np.linalg.norm(t[:, 0] - x2 / np.linalg.norm(x2)) < 1e-10
 
 
+def test_oracle_jada_minres_equals_gmres_on_symmetric_operators():
+    """the numpy restatement of PHIST's MINRES: for a symmetric A the
+    projected operator is symmetric on the complement of Q, so MINRES and
+    GMRES minimise the residual over the same Krylov space and their iterates
+    after j steps coincide (restarted too); converged runs solve the
+    systems"""
+    from oracle import oracle as O
+    rng = np.random.default_rng(2)
+    n = 60
+    A = rng.standard_normal((n, n))
+    A = A + A.T + 10 * np.eye(n)
+    Q = np.linalg.qr(rng.standard_normal((n, 3)))[0]
+    R = rng.standard_normal((n, 2))
+    R -= Q @ (Q.T @ R)
+    P = np.eye(n) - Q @ Q.T
+    for j, m in ((1, 20), (3, 20), (8, 20), (10, 4)):
+        tm, cm = O.jada_minres(A, Q, R, [0.5, -0.3], [1e-30, 1e-30], j, m)
+        tg, cg = O.jada_gmres(A, Q, R, [0.5, -0.3], [1e-30, 1e-30], j, m)
+        assert not cm.any() and not cg.any()
+        assert np.linalg.norm(tm - tg) < 1e-9, (j, m, np.linalg.norm(tm - tg))
+    # restarted MINRES needs the basis of its cap here: Lanczos without
+    # reorthogonalisation converges late on this indefinite operator (about
+    # 80 steps unrestarted for n = 60), and a restart after 60 steps keeps
+    # only a 1e-4 residual
+    t, conv = O.jada_minres(A, Q, R, [0.5, 1.0], [1e-10, 1e-10], 400, 63)
+    assert conv.all()
+    for s, sg in enumerate((0.5, 1.0)):
+        y = P @ (A - sg * np.eye(n)) @ t[:, s]
+        a = (y @ R[:, s]) / (y @ y)
+        assert np.linalg.norm(a * y - R[:, s]) < 1e-9 * np.linalg.norm(R[:, s])
+
+
 def test_oracle_carp_cgmn_solves_shifted_systems():
     """the CGMN restatement converges to the dense solutions of
     (A - sigma_j I) x_j = b_j (small honeycomb, shifts outside the spectrum)"""
