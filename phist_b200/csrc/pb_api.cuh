@@ -1328,15 +1328,23 @@ bool mvsd_gram_dmma_launch(RowGemmArgs<double>& a)
     mV = mA;
   }
   const size_t smem = 8 * ((size_t)CSZ + (size_t)S * R * AP + (size_t)S * VSZ + (size_t)R * PT) + 8 * S;
-  const int grid = (int)std::min<int64_t>(ceil_div(a.n, R), (int64_t)rt().num_sms() * 2);
+  // one wave of as many blocks as fit an SM (shared memory allows 4 at
+  // width 8, 2 from width 16 on)
+  auto kern = k_mvsd_gram_dmma<BM, BK, MV, R, S, GM>;
+  set_smem(kern, smem);
+  static std::atomic<int> occ{0};
+  if (occ.load() == 0) {
+    int o = 0;
+    PB_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&o, kern, BLK_BS, smem));
+    occ.store(std::max(1, o));
+  }
+  const int grid = (int)std::min<int64_t>(ceil_div(a.n, R), (int64_t)rt().num_sms() * occ.load());
   const int gm = (GM == GM_WW) ? a.k : a.mv;
   const int nout = gm * a.k;
   a.part = (double*)rt().scratch(sizeof(double) * (size_t)grid * nout);
   a.counter = rt().counters();
   const bool ext = nout >= 64 && grid > 1;
   a.R = ext ? -1 : R;
-  auto kern = k_mvsd_gram_dmma<BM, BK, MV, R, S, GM>;
-  set_smem(kern, smem);
   kern<<<grid, BLK_BS, smem, stream()>>>(a, mA, mV, rt().device_error_word());
   PB_LAUNCH_CHECK();
   if (ext) {
