@@ -1178,6 +1178,31 @@ void launch_mvTmv(int64_t n, int m, int k, T alpha, const T* V, int64_t ldv, con
   MvTmvArgs<T> a;
   a.n = n; a.m = m; a.k = k; a.V = V; a.ldv = ldv; a.W = W; a.ldw = ldw;
   a.alpha = alpha; a.beta = beta; a.Cd = Cd; a.ldc = ldc;
+  if constexpr (std::is_same<T, double>::value) {
+    // FP64 blocks of exactly 4 columns on 32-byte row boundaries: thread per
+    // row with 256-bit loads (n = 2,097,152: 38.9 us against 51.7 us for
+    // the staged tile kernel; at 8 columns the tile kernel stays faster,
+    // 68.9 against 71.8 us)
+    const bool a32 = ((uintptr_t)V & 31u) == 0 && ((uintptr_t)W & 31u) == 0 && ldv % 4 == 0 && ldw % 4 == 0;
+    if (rt().spmv_v256 && a32 && m == 4 && k == 4 && n > 0) {
+      static std::atomic<int> occ[1];
+      auto run = [&](auto kern, std::atomic<int>& o) {
+        if (o.load() == 0) {
+          int b = 0;
+          PB_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&b, kern, 256, 0));
+          o.store(std::max(1, b));
+        }
+        const int grid = (int)std::max<int64_t>(1, std::min<int64_t>(ceil_div(n, 256), (int64_t)rt().num_sms() * o.load()));
+        a.part = (T*)rt().scratch(sizeof(T) * (size_t)grid * m * k);
+        a.counter = rt().counters();
+        a.R = 0;
+        kern<<<grid, 256, 0, stream()>>>(a);
+        PB_LAUNCH_CHECK();
+      };
+      run(k_mvTmv_v4<4, 4, 4>, occ[0]);
+      return;
+    }
+  }
   if (m <= 64 && k <= 64 && vec_ok(V, ldv, m) && vec_ok(W, ldw, k)) {
     // multi-stage asynchronously staged row tiles, widths padded to 4..64
     mvtmv_async<T>(a, n, pad_width5(m), pad_width5(k));

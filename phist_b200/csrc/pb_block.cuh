@@ -366,6 +366,56 @@ __global__ void __launch_bounds__(256) k_mvTmv_reg(MvTmvArgs<T> a)
   last_block_reduce<T>(a.part, M * K, gridDim.x, a.counter, a.Cd, 1, M, a.ldc, a.alpha, a.beta, a.m, a.k);
 }
 
+// Thin blocks of exactly M and K columns (multiples of 4) whose rows start
+// on 32-byte boundaries: one thread per row, each row of V and W read with
+// 256-bit loads (ld.global.nc.v4.f64, 4 doubles), UNR rows of a thread in
+// flight before their FMAs; the same fixed-order reductions as k_mvTmv_reg.
+__device__ __forceinline__ void ld4_nc(const double* p, double* o)
+{
+  asm volatile("ld.global.nc.v4.f64 {%0, %1, %2, %3}, [%4];\n"
+               : "=d"(o[0]), "=d"(o[1]), "=d"(o[2]), "=d"(o[3])
+               : "l"(p));
+}
+
+template <int M, int K, int UNR>
+__global__ void __launch_bounds__(256) k_mvTmv_v4(MvTmvArgs<double> a)
+{
+  double acc[M * K];
+#pragma unroll
+  for (int q = 0; q < M * K; q++) acc[q] = 0.0;
+  const int64_t stride = (int64_t)gridDim.x * blockDim.x;
+  int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
+  for (; i + (UNR - 1) * stride < a.n; i += UNR * stride) {
+    double v[UNR][M], w[UNR][K];
+#pragma unroll
+    for (int u = 0; u < UNR; u++) {
+#pragma unroll
+      for (int c = 0; c < M; c += 4) ld4_nc(a.V + (i + u * stride) * a.ldv + c, &v[u][c]);
+#pragma unroll
+      for (int c = 0; c < K; c += 4) ld4_nc(a.W + (i + u * stride) * a.ldw + c, &w[u][c]);
+    }
+#pragma unroll
+    for (int u = 0; u < UNR; u++)
+#pragma unroll
+      for (int q = 0; q < K; q++)
+#pragma unroll
+        for (int p = 0; p < M; p++) acc[p + q * M] += v[u][p] * w[u][q];
+  }
+  for (; i < a.n; i += stride) {
+    double v[M], w[K];
+#pragma unroll
+    for (int c = 0; c < M; c += 4) ld4_nc(a.V + i * a.ldv + c, &v[c]);
+#pragma unroll
+    for (int c = 0; c < K; c += 4) ld4_nc(a.W + i * a.ldw + c, &w[c]);
+#pragma unroll
+    for (int q = 0; q < K; q++)
+#pragma unroll
+      for (int p = 0; p < M; p++) acc[p + q * M] += v[p] * w[q];
+  }
+  block_partial<double, M * K>(acc, a.part, M * K);
+  last_block_reduce<double>(a.part, M * K, gridDim.x, a.counter, a.Cd, 1, M, a.ldc, a.alpha, a.beta, a.m, a.k);
+}
+
 // row-local products for m, k, mv <= 8 (modes and Gram as k_rowgemm)
 template <class T, int M, int K, int MV>
 __global__ void __launch_bounds__(256) k_rowgemm_reg(RowGemmArgs<T> a)
