@@ -342,6 +342,109 @@ __global__ void k_lz_coef(const T* __restrict__ O1, const T* __restrict__ Nf, in
   hL[j * k + s] = (T)alpha;
 }
 
+// MINRES step with the projection P = I - Q Q' fused into its two passes
+// (thread per (row, system) as k_gm_blk; Q n x nq, nq <= MQ, row-major with
+// leading dimension ldq):
+//   DOTS: out[i*k + s] = sum_r Q(r, i) w_s(r) (i < nq), out[nq*k + s] =
+//         sum_r V_j(r, s) w_s(r): the projection's Q'W and alpha from one
+//         read of W (alpha = V_j'W equals V_j'(P W) because V_j is
+//         orthogonal to Q)
+//   UPD:  w_s -= sum_i Q(r, i) c(i, s), then -= alpha_s V_j(r, s), then
+//         -= beta_s V_{j-1}(r, s) (PHIST's order: the operator's projection,
+//         then the Lanczos terms), out[s] = ||w_s||^2; coef = [c (nq*k) |
+//         alpha (k) | beta (k)]
+// Sums as in k_gm_blk (butterfly, warps in order, fixed-order last pass).
+template <class T, bool UPD, int MQ>
+__global__ void __launch_bounds__(256) k_lz_proj(int64_t n, int k, int kp, int nq, const T* __restrict__ Q,
+                                                 int64_t ldq, const T* __restrict__ Vj, const T* __restrict__ Vjm1,
+                                                 T* W, const T* __restrict__ coef, T* part, unsigned int* counter,
+                                                 T* out, int ext)
+{
+  const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
+  const int s = tid % kp;
+  const int nout = UPD ? k : (nq + 1) * k;
+  T cq[MQ], acc[MQ];
+  T ca = T(0), cb = T(0), aacc = T(0), nacc = T(0);
+#pragma unroll
+  for (int i = 0; i < MQ; i++) {
+    cq[i] = (UPD && i < nq && s < k) ? coef[i * k + s] : T(0);
+    acc[i] = T(0);
+  }
+  if (UPD && s < k) {
+    ca = coef[nq * k + s];
+    cb = Vjm1 ? coef[(nq + 1) * k + s] : T(0);
+  }
+  if (s < k) {
+    const int64_t rstep = (int64_t)gridDim.x * (256 / kp);
+    for (int64_t r = blockIdx.x * (int64_t)(256 / kp) + tid / kp; r < n; r += rstep) {
+      T q[MQ];
+#pragma unroll
+      for (int i = 0; i < MQ; i++) q[i] = (i < nq) ? Q[r * ldq + i] : T(0);
+      const T v = Vj[r * k + s];
+      T w = W[r * k + s];
+      if (UPD) {
+#pragma unroll
+        for (int i = 0; i < MQ; i++) w -= q[i] * cq[i];
+        w -= v * ca;
+        if (Vjm1) w -= Vjm1[r * k + s] * cb;
+        W[r * k + s] = w;
+        nacc += w * w;
+      } else {
+#pragma unroll
+        for (int i = 0; i < MQ; i++) acc[i] += q[i] * w;
+        aacc += v * w;
+      }
+    }
+  }
+#pragma unroll
+  for (int off = 16; off >= 1; off >>= 1) {
+    if (off < kp) break;
+    if (UPD) {
+      nacc += __shfl_xor_sync(0xffffffffu, nacc, off);
+    } else {
+#pragma unroll
+      for (int i = 0; i < MQ; i++)
+        if (i < nq) acc[i] += __shfl_xor_sync(0xffffffffu, acc[i], off);
+      aacc += __shfl_xor_sync(0xffffffffu, aacc, off);
+    }
+  }
+  __shared__ T red[8][GM_MAXOUT];
+  if (lane < kp && s < k) {
+    if (UPD) {
+      red[warp][s] = nacc;
+    } else {
+#pragma unroll
+      for (int i = 0; i < MQ; i++)
+        if (i < nq) red[warp][i * k + s] = acc[i];
+      red[warp][nq * k + s] = aacc;
+    }
+  }
+  __syncthreads();
+  for (int o = tid; o < nout; o += 256) {
+    T a = T(0);
+    for (int w8 = 0; w8 < 8; w8++) a += red[w8][o];
+    part[(int64_t)blockIdx.x * nout + o] = a;
+  }
+  if (ext) return;  // second pass: k_reduce_partials
+  last_block_reduce<T>(part, nout, gridDim.x, counter, out, 1, nout, 0, T(1), T(0));
+}
+
+// Lanczos coefficients of the fused step: alpha_s = O[nq*k + s], beta_s =
+// sqrt(Nf_s) of the previous step (j > 0); column j of H as k_lz_coef;
+// beta stored at O[(nq+1)*k + s] for the update pass
+template <class T>
+__global__ void k_lz_coef_proj(T* O, int nq, const T* __restrict__ Nf, int j, int k, int m, double* H)
+{
+  const int s = threadIdx.x;
+  if (s >= k) return;
+  const double alpha = (double)O[nq * k + s];
+  const double beta = j > 0 ? sqrt(fmax((double)Nf[s], 0.0)) : 0.0;
+  for (int i = 0; i + 1 < j; i++) H[((int64_t)i * m + j) * k + s] = 0.0;
+  if (j > 0) H[((int64_t)(j - 1) * m + j) * k + s] = beta;
+  H[((int64_t)j * m + j) * k + s] = alpha;
+  O[(nq + 1) * k + s] = (T)beta;
+}
+
 // out[o] = sum over blocks of part[b*nout + o] (k_reduce_partials) unless
 // *skip == 0
 template <class T>
@@ -417,6 +520,36 @@ void gm_update(int64_t n, int k, int J, const T* V, T* W, const T* h, const int*
   for (int i0 = 0; i0 < J; i0 += cj) gm_blk<T, true, false>(n, k, i0, std::min(J, i0 + cj), V, W, h, skip, nrm);
 }
 
+// one launch of k_lz_proj (MQ: nq rounded up to 4, 8, 16 or 32)
+template <class T, bool UPD>
+void lz_proj(int64_t n, int k, int nq, const T* Q, int64_t ldq, const T* Vj, const T* Vjm1, T* W, const T* coef,
+             T* out)
+{
+  const int kp = k <= 1 ? 1 : k <= 2 ? 2 : k <= 4 ? 4 : k <= 8 ? 8 : k <= 16 ? 16 : 32;
+  const int nout = UPD ? k : (nq + 1) * k;
+  auto launch = [&](auto kern, std::atomic<int>& occ) {
+    if (occ.load() == 0) {
+      int b = 0;
+      PB_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&b, kern, 256, 0));
+      occ.store(std::max(1, b));
+    }
+    const int grid = (int)std::max<int64_t>(1, std::min<int64_t>(ceil_div(n, 256 / kp), (int64_t)rt().num_sms() * occ.load()));
+    const int ext = (nout >= 32 && grid > 32) ? 1 : 0;
+    T* part = (T*)rt().scratch(sizeof(T) * (size_t)grid * nout);
+    kern<<<grid, 256, 0, stream()>>>(n, k, kp, nq, Q, ldq, Vj, Vjm1, W, coef, part, rt().counters(), out, ext);
+    PB_LAUNCH_CHECK();
+    if (ext) {
+      k_gm_reduce_if<T><<<(nout + 31) / 32, 256, 0, stream()>>>(part, grid, nout, out, nullptr);
+      PB_LAUNCH_CHECK();
+    }
+  };
+  static std::atomic<int> occ[4];
+  if (nq <= 4) launch(k_lz_proj<T, UPD, 4>, occ[0]);
+  else if (nq <= 8) launch(k_lz_proj<T, UPD, 8>, occ[1]);
+  else if (nq <= 16) launch(k_lz_proj<T, UPD, 16>, occ[2]);
+  else launch(k_lz_proj<T, UPD, 32>, occ[3]);
+}
+
 }  // namespace
 
 // W = alpha V C + beta W on device operands (C col-major m x k, ld ldc)
@@ -469,6 +602,10 @@ int jada_krylov(const SparseMat<T>* A, const Mvec<T>* Q, const Mvec<T>* R, const
   DBuf<double> H((size_t)(m + 1) * m * k), cs((size_t)m * k), sn((size_t)m * k), g((size_t)(m + 1) * k), bnorm(k);
   DBuf<int> conv(k), jcount(k), reorth(1);
   DBuf<T> O1((size_t)(m + 2) * k), O2((size_t)(m + 2) * k), Nf(k), hL((size_t)(m + 1) * k);
+  // MINRES with a projection block of at most 32 columns: the projection is
+  // fused into the two Lanczos passes (k_lz_proj); P1 = [Q'W | alpha | beta]
+  const bool fuse = lanczos && nq > 0 && nq <= 32 && (nq + 1) * k <= GM_MAXOUT;
+  DBuf<T> P1((size_t)(nq + 2) * k);
   GmIndex gi;
   GmTol gt;
   for (int s = 0; s < k; s++) {
@@ -526,14 +663,22 @@ int jada_krylov(const SparseMat<T>* A, const Mvec<T>* Q, const Mvec<T>* R, const
       // W = P (A - sigma I) V_j
       raw_view(mVj, V.p + (int64_t)j * nk, n, k, k);
       spmv_general<T>(T(1), A, negsig.data(), &mVj, T(0), &mW, nullptr, nullptr, T(0), T(0), nullptr);
-      project();
+      if (!fuse) project();
       // Gram-Schmidt against V_0..V_j: h1 = V'W and ||W||^2; W -= V h1,
       // then h2 = V'W and ||W||^2 of the result (in one pass while the
       // blocks fit one launch); a second subtraction only where a norm fell
       // below 1/sqrt(2) of its value before (a device flag the second-pass
       // kernels read)
       const int J = j + 1;
-      if (lanczos) {
+      if (fuse) {
+        // [Q V_j]'W in one pass; W -= Q (Q'W) + V_j alpha + V_{j-1} beta and
+        // ||W||^2 into Nf in the next
+        const T* vj = V.p + (int64_t)j * nk;
+        lz_proj<T, false>(n, k, nq, Q->d(), Q->lda, vj, nullptr, W.p, nullptr, P1.p);
+        k_lz_coef_proj<T><<<1, 32, 0, stream()>>>(P1.p, nq, Nf.p, j, k, m, H.p);
+        PB_LAUNCH_CHECK();
+        lz_proj<T, true>(n, k, nq, Q->d(), Q->lda, vj, j > 0 ? vj - nk : nullptr, W.p, P1.p, Nf.p);
+      } else if (lanczos) {
         // alpha = V_j'W; W -= V_{j-1} beta + V_j alpha and ||W||^2 into Nf
         gm_blk<T, false, true>(n, k, j, J, V.p, W.p, nullptr, nullptr, O1.p);
         k_lz_coef<T><<<1, 32, 0, stream()>>>(O1.p, Nf.p, j, k, m, H.p, hL.p);
